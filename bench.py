@@ -1,0 +1,322 @@
+"""Benchmark of the PBILS hot path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload plain]
+
+Workload "plain": the reference's plain PBILS configuration, G(n=1000, p=0.5) from graph seed 1,
+k=5, population 128, tournament 5, perturbation 0.4, gww 0.1, 100 iterations with the early stop
+disabled (--early-stop 100), search seed 1 (rank r uses seed 1 + r).  One step = one full solve.
+Metric: PBILS iterations per second over the whole job (all ranks), plus LS moves/s.
+
+`value`: device time (CUDA events on the solver's stream) of solves on a graph and buffers already
+resident in HBM; L2 is flushed (a 256 MiB write) between timed steps, outside the events.
+`e2e`: the one-call public C ABI (ccb_pbils_solve) from a pinned host bitset to host labels, wall
+clock, every step paying the upload, allocation and the label read-back.
+Every step's objective is checked against the value the CPU oracle gives for this instance.
+
+Multi-GPU (torchrun): each rank solves its own instance (a different search seed) with no
+collective on the data path ("scaling": "weak"); the only collectives are the timing barrier and
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+PLAIN = dict(n=1000, density=0.5, graph_seed=1, k=5, population=128, tournament=5, perturbation=0.4, gww=0.1,
+             iterations=100, early_stop=100, seed=1)
+PLAIN_OBJECTIVE = {1: 234911}  # seed -> objective of the CPU oracle (and the reference binary)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["plain"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.txt), or None."""
+    path = os.path.join(REPO, "profiles", name + ".txt")
+    try:
+        with open(path) as fh:
+            m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", fh.read())
+            return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def reference_cpu_run(cfg, iterations, threads=0):
+    """One run of the reference's own CPU binary (oracle/_ref/cc_cpu); returns (solver seconds, f)."""
+    exe = os.path.join(REPO, "oracle", "_ref", "cc_cpu")
+    cmd = [exe, "--n", str(cfg["n"]), "--density", str(cfg["density"]), "--graph-seed", str(cfg["graph_seed"]),
+           "--k", str(cfg["k"]), "--pop", str(cfg["population"]), "--tournament", str(cfg["tournament"]),
+           "--perturb", str(cfg["perturbation"]), "--gww", str(cfg["gww"]), "--iters", str(iterations),
+           "--early-stop", str(cfg["early_stop"]), "--seed", str(cfg["seed"]), "--threads", str(threads),
+           "--no-verify"]
+    out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
+    t = float(re.search(r"time\s+best=([0-9.]+)s", out).group(1))
+    f = int(re.search(r"objective\s+min=(\d+)", out).group(1))
+    threads_used = int(re.search(r"threads\s+(\d+)", out).group(1))
+    return t, f, threads_used
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU implementation on this box's host cores."""
+    if rank != 0:
+        return
+    cfg = dict(PLAIN)
+    sample_iters = 10
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cc_cpu not built"}))
+        return
+    for _ in range(args.warmup):
+        reference_cpu_run(cfg, 2)
+    total_t, total_it, threads = 0.0, 0, 0
+    for _ in range(args.steps):
+        t, f, threads = reference_cpu_run(cfg, sample_iters)
+        total_t += t
+        total_it += sample_iters
+    value = total_it / total_t
+    line = {"metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "plain PBILS: ER(1000, 0.5, graph seed 1), k=5, pop=128, gww=0.1",
+                       "sample": f"{sample_iters} iterations per step (of 100)", "early_stop": 100},
+            "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
+                             "sample": f"{sample_iters} of the 100 iterations, --threads 0"},
+            "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    import cuda_graph_clustering_b200 as ccb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg = dict(PLAIN)
+    seed = cfg["seed"] + rank
+    graph = ccb.Graph.ErdosRenyi(cfg["n"], cfg["density"], cfg["graph_seed"])
+    params = ccb.PbilsParams(k=cfg["k"], population=cfg["population"], tournament=cfg["tournament"],
+                             perturbation=cfg["perturbation"], gww=cfg["gww"], iterations=cfg["iterations"],
+                             early_stop=cfg["early_stop"], seed=seed)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    dg = ccb.DeviceGraph(graph, stream=sh)
+    solver = ccb.Solver(dg, params)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    expected = PLAIN_OBJECTIVE.get(seed)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident solves -------------------------------------------------------------
+    for _ in range(args.warmup):
+        r = solver.pbils(params, stream=sh)
+    solver.set_profiling(False)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    results = []
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            events[i][0].record(stream)
+        results.append(solver.pbils(params, stream=sh, want_labels=False))
+        events[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = sum(step_ms)
+    iters = sum(r.iterations_done for r in results)
+    moves = sum(r.accepted_moves for r in results)
+    bit_exact = all(r.objective == expected for r in results) if expected is not None else None
+
+    # ---- per-kernel times (separate profiled pass: CUDA events around every launch) ----------
+    solver.set_profiling(True)
+    prof = solver.pbils(params, stream=sh, want_labels=False)
+    st = solver.stats()
+    solver.set_profiling(False)
+    descent_ms = st.descent_ms / max(st.descent_launches, 1)
+    launches_per_solve = st.descent_launches + st.rebuild_launches + st.record_launches + st.other_launches
+
+    # ---- end to end through the public one-call ABI ------------------------------------------
+    pinned = torch.empty(graph.bits.size, dtype=torch.int32, pin_memory=True)
+    pinned.numpy().view(np.uint32)[:] = graph.bits.reshape(-1)
+    pbits = pinned.numpy().view(np.uint32).reshape(graph.bits.shape)
+    g_pinned = ccb.Graph(graph.n, pbits, graph.edges)
+    for _ in range(max(1, args.warmup // 2)):
+        ccb.SolveGpu(g_pinned, params)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_ok = True
+    for _ in range(args.steps):
+        r = ccb.SolveGpu(g_pinned, params)
+        e2e_ok &= (expected is None or r.objective == expected)
+    e2e_s = time.perf_counter() - t0
+
+    # ---- max over ranks ------------------------------------------------------------------------
+    vals = torch.tensor([total_ms, e2e_s, float(iters), float(moves)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        mx = vals.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = vals.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        total_ms_all, e2e_all, iters_all, moves_all = mx[0].item(), mx[1].item(), sm[2].item(), sm[3].item()
+    else:
+        total_ms_all, e2e_all, iters_all, moves_all = total_ms, e2e_s, float(iters), float(moves)
+
+    if rank == 0:
+        n, k, pop = cfg["n"], cfg["k"], cfg["population"]
+        words = (n + 31) // 32
+        deg = 2.0 * graph.edges / n
+        ld = (n + 31) // 32 * 32
+        moves_per_launch = prof.accepted_moves / max(st.descent_launches, 1)
+        # algorithmic bytes of one descent launch: per move n*(k*2 + 1) + 4*words + 4*2*deg (scan of the
+        # state, the moved vertex's row, two G entries per neighbour), plus per slot the state copied in
+        # (k*ld*2 + ld) and the labels written out (ld)
+        per_move = n * (k * 2 + 1) + 4 * words + 8 * deg
+        per_launch = moves_per_launch * per_move + pop * (k * ld * 2 + 2 * ld)
+        peak, peak_kind = measured_peak_hbm()
+        achieved = per_launch / (descent_ms * 1e-3) / 1e9
+        traffic = profiled_traffic("k_descent_plain_n1000")
+        value = iters_all / (total_ms_all * 1e-3)
+        cpu = None
+        if not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
+            t, f, threads = reference_cpu_run(cfg, 20)
+            cpu = {"value": 20 / t, "unit": "iter/s", "cores": threads, "kind": "reference",
+                   "sample": "20 of the 100 iterations of the same instance and seed, --threads 0"}
+        line = {
+            "metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "config": {"workload": "plain PBILS: ER(n=1000, p=0.5, graph seed 1), k=5, pop=128, tournament 5, "
+                                   "perturb 0.4, gww 0.1, 100 iterations (early stop off), seed 1 + rank",
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                       "kernel_plan": solver.describe()},
+            "ls_moves_per_s": moves_all / (total_ms_all * 1e-3),
+            "bit_exact": bit_exact,
+            "objective": results[0].objective,
+            "e2e": {"value": iters_all / e2e_all, "unit": "iter/s",
+                    "h2d_bytes_per_step": int(graph.bits.nbytes), "d2h_bytes_per_step": int(4 * n + 48),
+                    "bit_exact": e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_descent", "algorithmic_bytes_per_launch": per_launch,
+                         "avg_launch_ms": descent_ms},
+            "kernel_ms_per_solve": {"descent": st.descent_ms, "rebuild": st.rebuild_ms, "record": st.record_ms,
+                                    "other": st.other_ms},
+            "gpu_launches": int(launches_per_solve * args.steps),
+            "clocks": clock_info,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

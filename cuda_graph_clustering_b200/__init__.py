@@ -1,0 +1,229 @@
+"""B200-native PBILS k-correlation clustering: Python mirror of the reference's solver interface.
+
+The reference (oQaris/cuda_graph_clustering) exposes ``cc::SolveGpu``,
+``cc::SolveNeighborhoodGpu`` and ``cc::SolveNeighborhoodWithManyLocalSearchesGpu`` over
+``cc::Graph`` and ``cc::PbilsParams`` (include/cc_gpu.hpp:10-20, include/cc_pbils.hpp:26-59).  This
+module keeps those names, argument meanings and errors (``RuntimeError`` with the reference's
+message) over the C ABI of ``libccb.so`` (include/ccb.h).  Every compute call runs the hand-written
+sm_100a kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from ._native import (CcbError, CcbParams, CcbResult, CcbKernelStats, LS_AUTO, LS_GLOBAL, LS_SHARED, LS_WIDE,
+                      MAX_CLUSTERS, MAX_VERTICES_NARROW, MAX_VERTICES_WIDE, check, lib)
+
+__all__ = ["Graph", "PbilsParams", "PbilsResult", "SolveGpu", "SolveNeighborhoodGpu",
+           "SolveNeighborhoodWithManyLocalSearchesGpu", "DeviceGraph", "Solver", "CcbError", "LS_AUTO", "LS_GLOBAL",
+           "LS_SHARED", "LS_WIDE", "MAX_CLUSTERS", "kMaxClusters"]
+
+kMaxClusters = MAX_CLUSTERS  # include/cc_gpu.hpp:10
+
+
+def words_per_row(n: int) -> int:
+    """cc::Graph's row length: max(1, ceil(n / 32)) words (src/cc_graph.cpp:149-153)."""
+    return 1 if n == 0 else (n + 31) // 32
+
+
+class Graph:
+    """Undirected, unweighted, loop-free graph as the reference's bitset (include/cc_graph.hpp:15-59)."""
+
+    def __init__(self, n: int = 0, bits: np.ndarray | None = None, edges: int | None = None):
+        self.n = int(n)
+        w = words_per_row(self.n)
+        if bits is None:
+            bits = np.zeros((self.n, w), np.uint32)
+        self.bits = np.ascontiguousarray(bits, dtype=np.uint32).reshape(self.n, -1 if self.n else w)
+        if self.bits.shape[1] < (self.n + 31) // 32:
+            raise ValueError("rows shorter than ceil(n / 32) words")
+        self.edges = int(edges) if edges is not None else int(sum(int(x).bit_count() for x in self.bits.ravel())) // 2
+
+    def Size(self) -> int:
+        return self.n
+
+    def WordsPerRow(self) -> int:
+        return self.bits.shape[1]
+
+    def EdgeCount(self) -> int:
+        return self.edges
+
+    def IsJoined(self, i: int, j: int) -> bool:
+        return bool((int(self.bits[i, j // 32]) >> (j % 32)) & 1)
+
+    def AddEdge(self, i: int, j: int) -> None:
+        if i == j or self.IsJoined(i, j):
+            return
+        self.bits[i, j // 32] |= np.uint32(1 << (j % 32))
+        self.bits[j, i // 32] |= np.uint32(1 << (i % 32))
+        self.edges += 1
+
+    def Density(self) -> float:
+        pairs = self.n * (self.n - 1) / 2
+        return self.edges / pairs if pairs > 0 else 0.0
+
+    @staticmethod
+    def ErdosRenyi(n: int, density: float, seed: int) -> "Graph":
+        """Graph::ErdosRenyi (src/cc_graph.cpp:168-177), generated by libccb on the host."""
+        w = words_per_row(n)
+        bits = np.zeros((max(n, 1), w), np.uint32)
+        edges = lib().ccb_generate_erdos_renyi(n, density, seed, bits.ctypes.data, w)
+        return Graph(n, bits[:n], edges)
+
+    @staticmethod
+    def Planted(n: int, parts: int, p_in: float, p_out: float, flip: float, seed: int,
+                shuffle_split: bool = False) -> tuple["Graph", np.ndarray]:
+        """Seeded planted partition (this project's generator; no counterpart in the reference)."""
+        w = words_per_row(n)
+        bits = np.zeros((max(n, 1), w), np.uint32)
+        comm = np.zeros(max(n, 1), np.int32)
+        edges = lib().ccb_generate_planted(n, parts, int(shuffle_split), p_in, p_out, flip, seed, bits.ctypes.data,
+                                           w, comm.ctypes.data)
+        return Graph(n, bits[:n], edges), comm[:n]
+
+
+@dataclass
+class PbilsParams:
+    """cc::PbilsParams (include/cc_pbils.hpp:26-49) with its defaults."""
+
+    k: int = 2
+    population: int = 128
+    tournament: int = 5
+    iterations: int = 100
+    early_stop: int = 6
+    perturbation: float = 0.4
+    gww: float = 0.1
+    threads: int = 1
+    seed: int = 1
+    time_limit_sec: float = 0.0
+    verbose: bool = False
+    ls_kernel: int = LS_AUTO
+
+    def to_c(self) -> CcbParams:
+        return CcbParams(self.k, self.population, self.tournament, self.iterations, self.early_stop,
+                         self.perturbation, self.gww, self.threads, self.seed, self.time_limit_sec,
+                         int(bool(self.verbose)), self.ls_kernel)
+
+
+@dataclass
+class PbilsResult:
+    """cc::PbilsResult (include/cc_pbils.hpp:51-59)."""
+
+    objective: int = -1
+    labels: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    iterations_done: int = 0
+    clusters_used: int = 0
+    seconds: float = 0.0
+    local_searches: int = 0
+    accepted_moves: int = 0
+
+    @staticmethod
+    def from_c(r: CcbResult, labels: np.ndarray) -> "PbilsResult":
+        return PbilsResult(int(r.objective), labels, int(r.iterations_done), int(r.clusters_used), float(r.seconds),
+                           int(r.local_searches), int(r.accepted_moves))
+
+
+def _run(fn, graph: Graph, params: PbilsParams, *extra) -> PbilsResult:
+    labels = np.zeros(max(graph.n, 1), np.int32)
+    res = CcbResult()
+    p = params.to_c()
+    status = fn(graph.bits.ctypes.data if graph.n else None, graph.n, graph.WordsPerRow(), graph.edges, C.byref(p),
+                *extra, labels.ctypes.data, C.byref(res))
+    check(status)
+    return PbilsResult.from_c(res, labels[: graph.n])
+
+
+def SolveGpu(graph: Graph, params: PbilsParams) -> PbilsResult:
+    """cc::SolveGpu (cuda/cc_pbils_gpu.cu:441-454)."""
+    return _run(lib().ccb_pbils_solve, graph, params)
+
+
+def SolveNeighborhoodGpu(graph: Graph, params: PbilsParams) -> PbilsResult:
+    """cc::SolveNeighborhoodGpu (cuda/cc_pbils_gpu.cu:456-458)."""
+    return _run(lib().ccb_neighborhood_solve, graph, params, 0)
+
+
+def SolveNeighborhoodWithManyLocalSearchesGpu(graph: Graph, params: PbilsParams) -> PbilsResult:
+    """cc::SolveNeighborhoodWithManyLocalSearchesGpu (cuda/cc_pbils_gpu.cu:460-462)."""
+    return _run(lib().ccb_neighborhood_solve, graph, params, 1)
+
+
+class DeviceGraph:
+    """A graph kept on the device across solves (ccb_graph_upload / ccb_graph_from_device)."""
+
+    def __init__(self, graph: Graph | None = None, stream: int = 0, device_ptr: int | None = None, n: int = 0,
+                 words: int = 0, edges: int = 0):
+        h = C.c_void_p()
+        if graph is not None:
+            check(lib().ccb_graph_upload(graph.bits.ctypes.data if graph.n else None, graph.n, graph.WordsPerRow(),
+                                         graph.edges, stream or None, C.byref(h)))
+            self.n, self.edges = graph.n, graph.edges
+        else:
+            check(lib().ccb_graph_from_device(device_ptr, n, words, edges, stream or None, C.byref(h)))
+            self.n, self.edges = n, edges
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ccb_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """Reusable buffers and kernel plan for (graph, k, population, ls_kernel) (ccb_solver_*)."""
+
+    def __init__(self, graph: DeviceGraph, params: PbilsParams):
+        h = C.c_void_p()
+        p = params.to_c()
+        check(lib().ccb_solver_create(graph.handle, C.byref(p), C.byref(h)))
+        self.handle = h
+        self.graph = graph
+        self.n = graph.n
+
+    def describe(self) -> str:
+        return lib().ccb_solver_describe(self.handle).decode()
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().ccb_solver_set_profiling(self.handle, int(on)))
+
+    def stats(self) -> CcbKernelStats:
+        s = CcbKernelStats()
+        check(lib().ccb_solver_stats(self.handle, C.byref(s)))
+        return s
+
+    def pbils(self, params: PbilsParams, stream: int = 0, want_labels: bool = True) -> PbilsResult:
+        labels = np.zeros(max(self.n, 1), np.int32)
+        res = CcbResult()
+        p = params.to_c()
+        check(lib().ccb_solver_pbils(self.handle, C.byref(p), stream or None,
+                                     labels.ctypes.data if want_labels else None, C.byref(res)))
+        return PbilsResult.from_c(res, labels[: self.n])
+
+    def neighborhood(self, params: PbilsParams, local_search: bool, stream: int = 0) -> PbilsResult:
+        labels = np.zeros(max(self.n, 1), np.int32)
+        res = CcbResult()
+        p = params.to_c()
+        check(lib().ccb_solver_neighborhood(self.handle, C.byref(p), int(local_search), stream or None,
+                                            labels.ctypes.data, C.byref(res)))
+        return PbilsResult.from_c(res, labels[: self.n])
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ccb_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

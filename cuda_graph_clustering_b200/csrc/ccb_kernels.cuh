@@ -1,0 +1,444 @@
+// Kernels of the PBILS iteration (one launch each, stream-ordered, no host round trip):
+//
+//   k_init_labels      initial population labels                       (cc_population_kernels.cuh:26-30)
+//   k_rebuild          [perturb | copy | neighbourhood labels] + G = A*Z, sizes, f per slot
+//                                                                      (cc_population_kernels.cuh:32-136)
+//   k_descent          tournament select + steepest descent per slot   (cc_local_search.cuh:15-121,
+//                                                                       cc_population_kernels.cuh:140-161)
+//   k_record           record, stall / early stop, GWW source map      (cc_pbils_gpu.cu:325-345,
+//                                                                       cc_pbils.hpp:69-78)
+//   k_degrees          vertex degrees                                  (cc_population_kernels.cuh:82-89)
+//
+// The iteration is  descent(it) -> record(it) -> rebuild(perturb, it):  descent reads the current
+// population and writes the next one, rebuild reads the next one and writes the current one back, so
+// the two buffers never swap.  The GWW copy (cc_pbils_cpu.cpp:234-239) is folded into the rebuild:
+// slot s perturbs the labels of its source src[s], which is s except for the worst `copies` slots,
+// whose source is the matching winner.
+#pragma once
+
+#include <cstdint>
+
+#include "ccb_device.cuh"
+
+namespace ccb {
+
+enum RebuildMode : int {
+  kRebuildInPlace = 0,     // labels already in `cur`
+  kRebuildPerturb = 1,     // cur[s] = perturb(next[src[s]])
+  kRebuildCopy = 2,        // cur[s] = next[src[s]]            (no perturbation: k < 2 or p = 0)
+  kRebuildNeighborhood = 3 // cur[s] = {v, N(v)} vs rest with v = first + s
+};
+
+__global__ void k_mark_start(Control* ctl) {
+  ctl->t0_ns = GlobalTimerNs();
+}
+
+__global__ void k_degrees(const uint32_t* __restrict__ bits, int n, int words, int pitch, int32_t* degrees) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const uint32_t* row = bits + static_cast<size_t>(v) * pitch;
+  int d = 0;
+  for (int w = 0; w < words; ++w) d += __popc(row[w]);
+  degrees[v] = d;
+}
+
+// labels[slot][v] = InitialLabel(stream, slot * n + v, k) over a grid-stride loop.
+__global__ void k_init_labels(uint8_t* labels, int pop, int n, int ld, int k, uint64_t stream) {
+  const long long total = static_cast<long long>(pop) * n;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long slot = i / n;
+    const int v = static_cast<int>(i - slot * n);
+    labels[slot * ld + v] = static_cast<uint8_t>(InitialLabelOf(stream, static_cast<uint64_t>(i), k));
+  }
+}
+
+// Rebuild of one slot per block.  Phase 1 writes the slot's labels (per mode), phase 2 packs one bit
+// mask per cluster with warp ballots (masks live in a global scratch [slot][k][words], read back
+// through L1), phase 3 gives each warp whole rows: lanes stride over the row's words, AND it with the
+// masks of a chunk of clusters, count bits, and reduce across the warp in hardware.  The last
+// cluster's row of G is the degree minus the others, so only k - 1 masks are intersected.
+template <typename GainT, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_rebuild(GraphView gr, PopView<GainT> cur, const uint8_t* __restrict__ next_labels,
+                                                      const int32_t* __restrict__ src_map, uint32_t* __restrict__ masks,
+                                                      int k, int kpad, int ld, int mode, uint64_t stream,
+                                                      int iteration, float probability, int first,
+                                                      const Control* __restrict__ ctl) {
+  constexpr int kWarps = kThreads / kWarp;
+  constexpr int kChunk = 8;
+  __shared__ int s_sizes[kMaxK];
+  __shared__ long long s_sum[kWarps];
+  if (ctl != nullptr && (mode == kRebuildPerturb || mode == kRebuildCopy) && ctl->stop) return;
+
+  const int slot = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = gr.n;
+  const int words = gr.words;
+  uint8_t* labels = cur.labels + static_cast<size_t>(slot) * ld;
+
+  if (mode == kRebuildPerturb || mode == kRebuildCopy) {
+    const int src = src_map != nullptr ? src_map[slot] : slot;
+    const uint8_t* from = next_labels + static_cast<size_t>(src) * ld;
+    for (int v = tid; v < n; v += kThreads) {
+      int l = from[v];
+      if (mode == kRebuildPerturb) {
+        l = PerturbLabelOf(stream, static_cast<uint64_t>(slot) * n + v, iteration, l, k, probability);
+      }
+      labels[v] = static_cast<uint8_t>(l);
+    }
+  } else if (mode == kRebuildNeighborhood) {
+    const int center = first + slot;
+    const uint32_t* crow = gr.bits + static_cast<size_t>(center) * gr.pitch;
+    for (int v = tid; v < n; v += kThreads) labels[v] = (v == center || Bit(crow, v)) ? 0 : 1;
+  }
+  for (int c = tid; c < k; c += kThreads) s_sizes[c] = 0;
+  __syncthreads();
+
+  // Phase 2: masks of clusters 0 .. k-2 (and sizes of all clusters) by ballots over 32 labels.
+  uint32_t* my_masks = masks + static_cast<size_t>(slot) * k * words;
+  for (int w = warp; w < words; w += kWarps) {
+    const int v = w * kWarp + lane;
+    const int l = v < n ? labels[v] : -1;
+    for (int c = 0; c < k; ++c) {
+      const uint32_t m = __ballot_sync(kAllLanes, l == c);
+      if (lane == (c % kWarp)) {
+        if (c < k - 1) my_masks[static_cast<size_t>(c) * words + w] = m;
+        if (m) atomicAdd(&s_sizes[c], __popc(m));
+      }
+    }
+  }
+  __syncthreads();
+
+  // Phase 3: G rows.
+  GainT* g = cur.g + static_cast<size_t>(slot) * k * ld;
+  long long intra_twice = 0;
+  for (int v = warp; v < n; v += kWarps) {
+    const uint32_t* row = gr.bits + static_cast<size_t>(v) * gr.pitch;
+    int rest = gr.degrees[v];
+    const int own = labels[v];
+    int g_own = 0;
+    for (int c0 = 0; c0 < k - 1; c0 += kChunk) {
+      int acc[kChunk];
+#pragma unroll
+      for (int i = 0; i < kChunk; ++i) acc[i] = 0;
+      for (int w = lane; w < words; w += kWarp) {
+        const uint32_t a = __ldg(row + w);
+#pragma unroll
+        for (int i = 0; i < kChunk; ++i) {
+          if (c0 + i < k - 1) acc[i] += __popc(a & my_masks[static_cast<size_t>(c0 + i) * words + w]);
+        }
+      }
+      int mine = 0;
+#pragma unroll
+      for (int i = 0; i < kChunk; ++i) {
+        if (c0 + i < k - 1) {
+          const int total = __reduce_add_sync(kAllLanes, static_cast<unsigned>(acc[i]));
+          rest -= total;
+          if (lane == i) mine = total;
+          if (own == c0 + i) g_own = total;
+        }
+      }
+      if (lane < kChunk && c0 + lane < k - 1) g[static_cast<size_t>(c0 + lane) * ld + v] = static_cast<GainT>(mine);
+    }
+    if (lane == 0) {
+      g[static_cast<size_t>(k - 1) * ld + v] = static_cast<GainT>(rest);
+      intra_twice += (own == k - 1) ? rest : g_own;
+    }
+  }
+  const long long sum = BlockSum<kWarps>(intra_twice, s_sum);
+  if (tid == 0) {
+    int sizes_local[kMaxK];
+    for (int c = 0; c < k; ++c) sizes_local[c] = s_sizes[c];
+    cur.f[slot] = gr.edges + PairsInside(sizes_local, k) - sum;
+  }
+  for (int c = tid; c < k; c += kThreads) cur.sizes[static_cast<size_t>(slot) * kpad + c] = s_sizes[c];
+}
+
+// Arguments of the descent kernel (passed by value).
+template <typename GainT>
+struct DescentArgs {
+  GraphView gr;
+  PopView<GainT> cur;   // population the tournament draws from (read only)
+  PopView<GainT> next;  // labels and f written here; g used as scratch by the global-state form
+  Control* ctl;
+  int k;
+  int kpad;
+  int ld;
+  int key_bits;         // bit width of n: the vertex field of a move key
+  int population;       // slots in cur (tournament range)
+  int tournament;       // 0: slot s descends from cur[s] (Neighborhood), else tournament size
+  int iteration;
+  uint64_t select_stream;
+};
+
+// Steepest descent of one slot per block until no strictly improving single-vertex move remains.
+//
+// Thread t owns vertices u = t, t + T, t + 2T, ...  A move (v: from -> to) changes every vertex's
+// h_c(u) = size_c - 2 G_c(u) for c in {from, to}; the gain of moving u from a to c is
+// h_c - h_a + 1 (cc_math.hpp:75-77).  Per move each thread scans its vertices for its best (gain, u)
+// with the target of u as payload, the block takes the minimum in one barrier (BlockArgMin), and
+// every thread applies the move to the G entries of its own vertices from row v of the adjacency.
+// Sizes live in a private copy per warp so that no second barrier is needed.
+//
+//   kSmemState: labels (1 B) and G of the slot sit in shared memory for the whole descent,
+//               otherwise in the slot's rows of `next` (global memory, L2 resident).
+//   kSmemRows:  the whole bitset is staged in shared memory (small n), otherwise rows come from L2.
+template <typename GainT, typename Key, bool kSmemState, bool kSmemRows, int kThreads>
+__global__ void __launch_bounds__(kThreads, 1) k_descent(DescentArgs<GainT> a) {
+  constexpr int kWarps = kThreads / kWarp;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_winner;
+  __shared__ int s_stop;
+
+  const int slot = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = a.gr.n;
+  const int k = a.k;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+
+  if (tid == 0) {
+    s_stop = a.ctl->stop;
+    if (!s_stop) {
+      const int64_t* f = a.cur.f;
+      s_winner = a.tournament > 0 ? TournamentWinner(a.select_stream, slot, a.iteration, a.population, a.tournament,
+                                                     [f](int i) { return f[i]; })
+                                  : slot;
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const int w = s_winner;
+
+  // Shared-memory carve-up (the host sizes it the same way): rows | G | labels | warp sizes | records.
+  unsigned char* p = smem;
+  const uint32_t* rows = a.gr.bits;
+  if constexpr (kSmemRows) {
+    uint32_t* srows = reinterpret_cast<uint32_t*>(p);
+    const size_t row_words = static_cast<size_t>(n) * a.gr.pitch;
+    const uint4* src = reinterpret_cast<const uint4*>(a.gr.bits);
+    uint4* dst = reinterpret_cast<uint4*>(srows);
+    for (size_t i = tid; i < row_words / 4; i += kThreads) dst[i] = __ldg(src + i);
+    rows = srows;
+    p += (row_words * 4 + 15) / 16 * 16;
+  }
+  GainT* g;
+  uint8_t* lab;
+  const size_t g_entries = static_cast<size_t>(k) * ld;
+  if constexpr (kSmemState) {
+    g = reinterpret_cast<GainT*>(p);
+    p += (g_entries * sizeof(GainT) + 15) / 16 * 16;
+    lab = p;
+    p += (ld + 15) / 16 * 16;
+  } else {
+    g = a.next.g + static_cast<size_t>(slot) * g_entries;
+    lab = a.next.labels + static_cast<size_t>(slot) * ld;
+  }
+  int* szw = reinterpret_cast<int*>(p);
+  p += static_cast<size_t>(kWarps) * a.kpad * sizeof(int);
+  MoveRecord<Key>* records = reinterpret_cast<MoveRecord<Key>*>((reinterpret_cast<uintptr_t>(p) + 15) / 16 * 16);
+
+  {
+    const uint4* gs = reinterpret_cast<const uint4*>(a.cur.g + static_cast<size_t>(w) * g_entries);
+    uint4* gd = reinterpret_cast<uint4*>(g);
+    for (size_t i = tid; i < g_entries * sizeof(GainT) / 16; i += kThreads) gd[i] = gs[i];
+    const uint4* ls = reinterpret_cast<const uint4*>(a.cur.labels + static_cast<size_t>(w) * ld);
+    uint4* ldst = reinterpret_cast<uint4*>(lab);
+    for (int i = tid; i < ld / 16; i += kThreads) ldst[i] = ls[i];
+    const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+    for (int i = tid; i < kWarps * k; i += kThreads) szw[(i / k) * a.kpad + i % k] = sizes[i % k];
+  }
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+  __syncthreads();
+
+  int* sz = szw + warp * a.kpad;
+  unsigned long long applied = 0;
+  int parity = 0;
+  while (true) {
+    // Scan: best target of each owned vertex (smallest h, lowest cluster on ties), then the best
+    // improving (gain, vertex) of the thread; vertices ascend, so strict < keeps the smallest vertex.
+    Key best = KeyTraits<Key>::kNone;
+    uint32_t payload = 0;
+    for (int u = tid; u < n; u += kThreads) {
+      const int from = lab[u];
+      int h_from = 0;
+      int h_best = 0x7fffffff;
+      int to = 0;
+      for (int c = 0; c < k; ++c) {
+        const int h = sz[c] - 2 * static_cast<int>(g[static_cast<size_t>(c) * ld + u]);
+        if (c == from) {
+          h_from = h;
+        } else if (h < h_best) {
+          h_best = h;
+          to = c;
+        }
+      }
+      const int delta = h_best - h_from + 1;
+      if (delta < 0) {
+        const Key key = PackMove<Key>(delta, u, bits);
+        if (key < best) {
+          best = key;
+          payload = static_cast<uint32_t>(from) | (static_cast<uint32_t>(to) << 8);
+        }
+      }
+    }
+    const MoveRecord<Key> m = BlockArgMin<Key, kWarps>(best, payload, records + parity * kWarps);
+    if (m.key == KeyTraits<Key>::kNone) break;
+    parity ^= 1;
+
+    const int v = MoveVertex(m.key, bits);
+    const int from = static_cast<int>(m.payload & 0xff);
+    const int to = static_cast<int>(m.payload >> 8);
+    if (lane == 0) {
+      sz[from] -= 1;
+      sz[to] += 1;
+    }
+    __syncwarp();
+    if (v % kThreads == tid) lab[v] = static_cast<uint8_t>(to);
+    const uint32_t* row = rows + static_cast<size_t>(v) * a.gr.pitch;
+    GainT* g_from = g + static_cast<size_t>(from) * ld;
+    GainT* g_to = g + static_cast<size_t>(to) * ld;
+    for (int u = tid; u < n; u += kThreads) {
+      if (Bit(row, u)) {
+        g_from[u] -= 1;
+        g_to[u] += 1;
+      }
+    }
+    objective += MoveDelta(m.key, bits);
+    ++applied;
+    // Every accepted move lowers f by at least one and f >= 0, so f of the start state bounds the
+    // number of moves; passing it means an inconsistent state, reported instead of looping on.
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      break;
+    }
+  }
+
+  if constexpr (kSmemState) {
+    uint4* ldst = reinterpret_cast<uint4*>(a.next.labels + static_cast<size_t>(slot) * ld);
+    const uint4* ls = reinterpret_cast<const uint4*>(lab);
+    for (int i = tid; i < ld / 16; i += kThreads) ldst[i] = ls[i];
+  }
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
+enum RecordMode : int {
+  kRecordInitial = 0,      // first offer (always taken), no iteration bookkeeping
+  kRecordIteration = 1,    // record + Progress::Next + GWW source map
+  kRecordNeighborhood = 2  // record only (strict improvement across batches)
+};
+
+struct RecordArgs {
+  const int64_t* f;       // objective per slot
+  const uint8_t* labels;  // labels per slot, leading dimension ld
+  int ld;
+  int n;
+  int count;              // slots to consider
+  Control* ctl;
+  uint8_t* record_labels; // n labels of the record
+  int mode;
+  int iteration;
+  int early_stop;
+  int copies;             // GWW: WinnerCopies(gww, population) (cc_pbils_cpu.cpp:168)
+  int32_t* src_map;       // GWW source of each slot's next member (null when copies == 0)
+  int32_t* order;         // scratch: slots by (f, slot)
+  TraceEntry* trace;      // progress log, one entry per iteration (may be null)
+  unsigned long long time_limit_ns;  // 0 = none
+};
+
+// One block.  The record takes the first slot of minimum f on a strict improvement
+// (cc_pbils_cpu.cpp:208-215); the stall counter and stop rule follow Progress::Next
+// (cc_pbils.hpp:69-78); the GWW map ranks slots by (f, slot) as RankSlots does
+// (cc_pbils_cpu.cpp:170-175) and sends the i-th best to the i-th worst for i < copies.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) k_record(RecordArgs a) {
+  constexpr int kWarps = kThreads / kWarp;
+  __shared__ long long s_f[kWarps];
+  __shared__ int s_slot[kWarps];
+  __shared__ int s_take;
+  __shared__ int s_best;
+  __shared__ int s_stop;
+  const int tid = threadIdx.x;
+  if (a.mode == kRecordIteration && a.ctl->stop) return;
+
+  long long bf = 0x7fffffffffffffffll;
+  int bs = 0x7fffffff;
+  for (int s = tid; s < a.count; s += kThreads) {
+    const long long f = a.f[s];
+    if (f < bf) {
+      bf = f;
+      bs = s;
+    }
+  }
+  for (int o = kWarp / 2; o > 0; o /= 2) {
+    const long long of = __shfl_xor_sync(kAllLanes, bf, o);
+    const int os = __shfl_xor_sync(kAllLanes, bs, o);
+    if (of < bf || (of == bf && os < bs)) {
+      bf = of;
+      bs = os;
+    }
+  }
+  if (tid % kWarp == 0) {
+    s_f[tid / kWarp] = bf;
+    s_slot[tid / kWarp] = bs;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    long long f = s_f[0];
+    int s = s_slot[0];
+    for (int w = 1; w < kWarps; ++w) {
+      if (s_f[w] < f || (s_f[w] == f && s_slot[w] < s)) {
+        f = s_f[w];
+        s = s_slot[w];
+      }
+    }
+    Control* c = a.ctl;
+    const int take = (a.mode == kRecordInitial) || !c->have_record || f < c->record_f;
+    if (take) {
+      c->record_f = f;
+      c->have_record = 1;
+      c->record_slot = s;
+    }
+    int stop = 0;
+    if (a.mode == kRecordIteration) {
+      c->iterations_done = a.iteration + 1;
+      c->stall = take ? 0 : c->stall + 1;
+      const unsigned long long now = GlobalTimerNs();
+      if (a.trace != nullptr) a.trace[a.iteration] = TraceEntry{c->record_f, c->stall, 0, now - c->t0_ns};
+      stop = c->stall >= a.early_stop || (a.time_limit_ns > 0 && now - c->t0_ns >= a.time_limit_ns);
+      if (stop) c->stop = 1;
+    }
+    s_take = take;
+    s_best = s;
+    s_stop = stop;
+  }
+  __syncthreads();
+  if (s_take) {
+    const uint8_t* src = a.labels + static_cast<size_t>(s_best) * a.ld;
+    for (int v = tid; v < a.n; v += kThreads) a.record_labels[v] = src[v];
+  }
+  if (a.mode != kRecordIteration || s_stop || a.copies <= 0) return;
+
+  for (int s = tid; s < a.count; s += kThreads) {
+    const long long f = a.f[s];
+    int rank = 0;
+    for (int t = 0; t < a.count; ++t) {
+      const long long ft = a.f[t];
+      rank += (ft < f) || (ft == f && t < s);
+    }
+    a.order[rank] = s;
+    a.src_map[s] = s;
+  }
+  __syncthreads();
+  for (int i = tid; i < a.copies; i += kThreads) a.src_map[a.order[a.count - 1 - i]] = a.order[i];
+}
+
+}  // namespace ccb

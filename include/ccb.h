@@ -1,0 +1,151 @@
+/*
+ * ccb.h — C ABI of the B200 PBILS k-correlation-clustering library (libccb.so).
+ *
+ * Plain pointers, sizes and status codes only: no C++ or framework types cross this boundary, so a
+ * C, C++ (cc::SolveGpu adapter), ctypes or cgo caller binds it directly.  Each entry point names the
+ * reference interface of oQaris/cuda_graph_clustering it replaces.
+ *
+ * Graph format (the reference's cc::Graph, include/cc_graph.hpp:15-59): n rows of `words_per_row`
+ * uint32 words, row-major; bit u of row v is set iff {u, v} is an edge; no self loops; the matrix is
+ * symmetric; bits past column n-1 are zero.  words_per_row >= ceil(n / 32) (the reference stores
+ * max(1, ceil(n / 32))).
+ *
+ * Errors: every function returns CCB_OK or a nonzero status; ccb_last_error() then gives the message
+ * (the text of the std::runtime_error the reference would throw, thread-local).  All work runs on the
+ * calling thread's current CUDA device.
+ */
+#ifndef CCB_H_
+#define CCB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ccb_status {
+  CCB_OK = 0,
+  CCB_ERR_INVALID = 1,       /* parameters rejected (bad k, population, gww, n, ...) */
+  CCB_ERR_DEVICE_MEMORY = 2, /* the run does not fit the free device memory / shared memory */
+  CCB_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  CCB_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (batched / serving paths) */
+  CCB_ERR_STATE = 5          /* handle misuse (null handle, queue full, ...) */
+};
+
+/* PbilsParams::LocalSearchKernel (include/cc_pbils.hpp:27-36). */
+enum ccb_ls_kernel { CCB_LS_AUTO = 0, CCB_LS_GLOBAL = 1, CCB_LS_SHARED = 2, CCB_LS_WIDE = 3 };
+
+/* cc::kMaxClusters (include/cc_gpu.hpp:10) and the packed-move vertex limit (cuda/cc_gpu_common.cuh:31-32). */
+#define CCB_MAX_CLUSTERS 64
+#define CCB_MAX_VERTICES_NARROW 32767
+#define CCB_MAX_VERTICES_WIDE (1 << 20)
+
+/* cc::PbilsParams (include/cc_pbils.hpp:26-49), field for field. */
+typedef struct ccb_params {
+  int32_t k;
+  int32_t population;
+  int32_t tournament;
+  int32_t iterations;
+  int32_t early_stop;
+  double perturbation;
+  double gww;
+  int32_t threads; /* CPU-only knob of the reference; accepted and ignored */
+  uint64_t seed;
+  double time_limit_sec; /* 0 = no limit */
+  int32_t verbose;
+  int32_t ls_kernel; /* enum ccb_ls_kernel */
+} ccb_params;
+
+/* cc::PbilsResult (include/cc_pbils.hpp:51-59) without the label vector, which the caller passes. */
+typedef struct ccb_result {
+  int64_t objective;
+  int32_t iterations_done;
+  int32_t clusters_used;
+  double seconds;
+  int64_t local_searches;
+  int64_t accepted_moves;
+} ccb_result;
+
+/* Message of the last failed call on this thread ("" after success). */
+const char* ccb_last_error(void);
+
+/* Fills the reference defaults: k 2, population 128, tournament 5, iterations 100, early_stop 6,
+ * perturbation 0.4, gww 0.1, threads 1, seed 1, no time limit, auto kernel (cc_pbils.hpp:32-43). */
+void ccb_params_init(ccb_params* params);
+
+/* ---- one-call solvers (host buffers in, host buffers out) ------------------------------------ */
+
+/* cc::SolveGpu (cuda/cc_pbils_gpu.cu:441-454).  labels_out: n int32 labels in [0, k). */
+int ccb_pbils_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                    const ccb_params* params, int32_t* labels_out, ccb_result* result);
+
+/* cc::SolveNeighborhoodGpu (local_search = 0) and cc::SolveNeighborhoodWithManyLocalSearchesGpu
+ * (local_search = 1) (cuda/cc_pbils_gpu.cu:456-462).  Uses params->k (must be 2), population (batch)
+ * and ls_kernel. */
+int ccb_neighborhood_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                           const ccb_params* params, int32_t local_search, int32_t* labels_out,
+                           ccb_result* result);
+
+/* ---- device-resident graphs and reusable solvers ----------------------------------------------
+ * The reference uploads the graph and allocates the population inside every solve
+ * (cuda/cc_pbils_gpu.cu:186-226).  These split that constructor so that a caller can keep the graph
+ * and buffers on the device across solves.  `stream` is a cudaStream_t (NULL = legacy default). */
+typedef struct ccb_graph ccb_graph;
+typedef struct ccb_solver ccb_solver;
+
+/* Copies a host bitset to the device (rows re-pitched to 16-byte multiples) and counts degrees. */
+int ccb_graph_upload(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges, void* stream,
+                     ccb_graph** out);
+/* Same from a device bitset (e.g. a framework tensor); the library keeps its own copy. */
+int ccb_graph_from_device(const uint32_t* device_bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                          void* stream, ccb_graph** out);
+int ccb_graph_size(const ccb_graph* graph, uint32_t* n, uint64_t* edges);
+void ccb_graph_destroy(ccb_graph* graph);
+
+/* Plans kernels and allocates buffers for (graph, k, population, ls_kernel); the solver can then run
+ * any number of solves with other seeds / iteration counts / gww / perturbation / tournament. */
+int ccb_solver_create(const ccb_graph* graph, const ccb_params* params, ccb_solver** out);
+/* Runs PBILS on the solver's graph.  Host labels_out (n int32) may be NULL.  Inputs already resident:
+ * no host-to-device copies happen inside. */
+int ccb_solver_pbils(ccb_solver* solver, const ccb_params* params, void* stream, int32_t* labels_out,
+                     ccb_result* result);
+/* Neighborhood enumerators on the solver's graph (k must be 2). */
+int ccb_solver_neighborhood(ccb_solver* solver, const ccb_params* params, int32_t local_search, void* stream,
+                            int32_t* labels_out, ccb_result* result);
+/* Text description of the plan ("generic, shared memory, 512 threads, ..."). */
+const char* ccb_solver_describe(const ccb_solver* solver);
+void ccb_solver_destroy(ccb_solver* solver);
+
+/* Per-kernel timing of the last solve (CUDA events around each launch; enabled by
+ * ccb_solver_set_profiling).  Times in milliseconds, launches counted. */
+typedef struct ccb_kernel_stats {
+  double descent_ms;
+  double rebuild_ms;
+  double record_ms;
+  double other_ms;
+  int64_t descent_launches;
+  int64_t rebuild_launches;
+  int64_t record_launches;
+  int64_t other_launches;
+} ccb_kernel_stats;
+int ccb_solver_set_profiling(ccb_solver* solver, int32_t enabled);
+int ccb_solver_stats(const ccb_solver* solver, ccb_kernel_stats* stats);
+
+/* ---- host instance generators (the instances of the reference's CLI and of the benchmarks) ----- */
+
+/* Graph::ErdosRenyi (src/cc_graph.cpp:168-177): bits holds n * words_per_row words. Returns edges. */
+uint64_t ccb_generate_erdos_renyi(uint32_t n, double density, uint64_t seed, uint32_t* bits,
+                                  uint32_t words_per_row);
+/* Seeded planted partition (no counterpart in the reference): `parts` communities, or with
+ * shuffle_split a seeded permutation split into halves; edge probability p_in inside a community,
+ * p_out across, then every pair flipped with probability `flip`.  community_out may be NULL. */
+uint64_t ccb_generate_planted(uint32_t n, int32_t parts, int32_t shuffle_split, double p_in, double p_out,
+                              double flip, uint64_t seed, uint32_t* bits, uint32_t words_per_row,
+                              int32_t* community_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCB_H_ */
