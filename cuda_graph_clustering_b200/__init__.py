@@ -227,3 +227,11 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+def evaluate_labelings(bits_ptr: int, n: int, words_per_row: int, edges: int, k: int, count: int, labels_ptr: int,
+                       f_ptr: int, sizes_ptr: int | None = None, g_ptr: int | None = None, stream: int = 0) -> None:
+    """Device recount of `count` labelings (ccb_evaluate_labelings); all pointers are device pointers."""
+    check(lib().ccb_evaluate_labelings(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr, sizes_ptr,
+                                       g_ptr, stream or None))
+

@@ -1,0 +1,141 @@
+// Device recount of labelings: objective f, cluster sizes and G = A*Z for a batch of labelings of one graph.
+// This is the GPU form of the reference's post-solve recount ObjectiveBitwise (src/cc_pbils_cpu.cpp:25-53,
+// run by the CLI at include/cc_cli.hpp:337-343) and of State::Rebuild (src/cc_pbils_cpu.cpp:74-95).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "ccb.h"
+#include "ccb_device.cuh"
+#include "ccb_error.h"
+
+namespace ccb {
+namespace {
+
+constexpr int kEvalThreads = 512;
+constexpr int kEvalChunk = 8;
+
+// One block per labeling.  Phase 1 packs a bit mask per cluster with warp ballots into `masks`
+// ([labeling][k][words], scratch) and counts cluster sizes; every mask word is written before it is
+// read, so the scratch needs no clearing.  Phase 2 gives each warp whole rows: lanes stride over the
+// row's words and count the bits shared with each cluster's mask, reduced across the warp in hardware.
+// A label outside [0, k) marks the labeling invalid: its f is written as -1.
+__global__ void __launch_bounds__(kEvalThreads)
+    k_evaluate(const uint32_t* __restrict__ bits, int n, int words, int pitch, long long edges, int k,
+               const int32_t* __restrict__ all_labels, uint32_t* __restrict__ masks, int64_t* __restrict__ f_out,
+               int32_t* __restrict__ sizes_out, int32_t* __restrict__ g_out) {
+  constexpr int kWarps = kEvalThreads / kWarp;
+  __shared__ int s_sizes[kMaxK];
+  __shared__ int s_bad;
+  __shared__ long long s_sum[kWarps];
+  const int sol = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int32_t* labels = all_labels + static_cast<size_t>(sol) * n;
+  uint32_t* my_masks = masks + static_cast<size_t>(sol) * k * words;
+  for (int c = tid; c < k; c += kEvalThreads) s_sizes[c] = 0;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+
+  for (int w = warp; w < words; w += kWarps) {
+    const int v = w * kWarp + lane;
+    const int l = v < n ? labels[v] : -1;
+    if (v < n && (l < 0 || l >= k)) s_bad = 1;
+    for (int c = 0; c < k; ++c) {
+      const uint32_t m = __ballot_sync(kAllLanes, l == c);
+      if (lane == (c % kWarp)) {
+        my_masks[static_cast<size_t>(c) * words + w] = m;
+        if (m) atomicAdd(&s_sizes[c], __popc(m));
+      }
+    }
+  }
+  __syncthreads();
+
+  long long intra_twice = 0;
+  for (int v = warp; v < n; v += kWarps) {
+    const uint32_t* row = bits + static_cast<size_t>(v) * pitch;
+    const int own = labels[v];
+    for (int c0 = 0; c0 < k; c0 += kEvalChunk) {
+      int acc[kEvalChunk];
+#pragma unroll
+      for (int i = 0; i < kEvalChunk; ++i) acc[i] = 0;
+      for (int w = lane; w < words; w += kWarp) {
+        const uint32_t a = __ldg(row + w);
+#pragma unroll
+        for (int i = 0; i < kEvalChunk; ++i)
+          if (c0 + i < k) acc[i] += __popc(a & my_masks[static_cast<size_t>(c0 + i) * words + w]);
+      }
+#pragma unroll
+      for (int i = 0; i < kEvalChunk; ++i) {
+        if (c0 + i < k) {
+          const int total = static_cast<int>(__reduce_add_sync(kAllLanes, static_cast<unsigned>(acc[i])));
+          if (lane == 0) {
+            if (g_out != nullptr) g_out[(static_cast<size_t>(sol) * k + c0 + i) * n + v] = total;
+            if (own == c0 + i) intra_twice += total;
+          }
+        }
+      }
+    }
+  }
+  const long long sum = BlockSum<kWarps>(intra_twice, s_sum);
+  if (tid == 0) {
+    long long pairs = 0;
+    for (int c = 0; c < k; ++c) pairs += static_cast<long long>(s_sizes[c]) * (s_sizes[c] - 1) / 2;
+    f_out[sol] = s_bad ? -1 : edges + pairs - sum;
+  }
+  if (sizes_out != nullptr) {
+    for (int c = tid; c < k; c += kEvalThreads) sizes_out[static_cast<size_t>(sol) * k + c] = s_sizes[c];
+  }
+}
+
+const char* CheckEvaluateArgs(const uint32_t* bits, uint32_t n, uint32_t words_per_row, int32_t k, int32_t count,
+                              const int32_t* labels, const int64_t* f_out) {
+  if (k < 1 || k > CCB_MAX_CLUSTERS) return "k must be in [1, 64]";
+  if (count < 0) return "count must be >= 0";
+  if (n > (uint32_t)CCB_MAX_VERTICES_WIDE) return "n exceeds 1048576, the range of the packed move";
+  if (n > 0 && words_per_row < (n + 31) / 32) return "words_per_row < ceil(n / 32)";
+  if (count > 0 && n > 0 && (bits == nullptr || labels == nullptr)) return "null bitset or labels";
+  if (count > 0 && f_out == nullptr) return "null f_out";
+  return nullptr;
+}
+
+int Report(int status, const char* message) {
+  SetLastError(message);
+  return status;
+}
+
+}  // namespace
+}  // namespace ccb
+
+using namespace ccb;
+
+extern "C" {
+
+int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges, int32_t k,
+                           int32_t count, const int32_t* labels, int64_t* f_out, int32_t* sizes_out, int32_t* g_out,
+                           void* stream) {
+  if (const char* why = CheckEvaluateArgs(bits, n, words_per_row, k, count, labels, f_out)) {
+    return Report(CCB_ERR_INVALID, why);
+  }
+  if (count == 0) return Report(CCB_OK, "");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int words = (int)((n + 31) / 32);
+  const size_t mask_bytes = sizeof(uint32_t) * (size_t)count * k * words;
+  uint32_t* masks = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (mask_bytes > 0) {
+    e = cudaMallocAsync(&masks, mask_bytes, st);
+    if (e != cudaSuccess) return Report(CCB_ERR_DEVICE_MEMORY, cudaGetErrorString(e));
+  }
+  k_evaluate<<<count, kEvalThreads, 0, st>>>(bits, (int)n, words, (int)words_per_row, (long long)edges, k, labels,
+                                             masks, f_out, sizes_out, g_out);
+  e = cudaGetLastError();
+  if (masks) cudaFreeAsync(masks, st);
+  if (e != cudaSuccess) return Report(CCB_ERR_CUDA, cudaGetErrorString(e));
+  return Report(CCB_OK, "");
+}
+
+}  // extern "C"
+

@@ -19,12 +19,23 @@
 #include <vector>
 
 #include "ccb.h"
+#include "ccb_error.h"
 #include "ccb_kernels.cuh"
 
 namespace ccb {
-namespace {
 
-thread_local std::string g_last_error;
+namespace {
+thread_local char g_last_error[1024];
+}  // namespace
+
+void SetLastError(const char* message) {
+  std::strncpy(g_last_error, message, sizeof(g_last_error) - 1);
+  g_last_error[sizeof(g_last_error) - 1] = '\0';
+}
+
+const char* LastError() { return g_last_error; }
+
+namespace {
 
 struct Failure {
   int status;
@@ -46,16 +57,16 @@ template <typename F>
 int Guard(F&& body) {
   try {
     body();
-    g_last_error.clear();
+    g_last_error[0] = '\0';
     return CCB_OK;
   } catch (const Failure& e) {
-    g_last_error = e.message;
+    SetLastError(e.message);
     return e.status;
   } catch (const std::bad_alloc&) {
-    g_last_error = "host memory exhausted";
+    SetLastError("host memory exhausted");
     return CCB_ERR_DEVICE_MEMORY;
   } catch (const std::exception& e) {
-    g_last_error = e.what();
+    SetLastError(e.what());
     return CCB_ERR_INVALID;
   }
 }
@@ -698,7 +709,7 @@ void CheckSolverMatches(const ccb_solver* s, const ccb_params& p) {
 // ------------------------------------------------------------------------------------------------
 extern "C" {
 
-const char* ccb_last_error(void) { return g_last_error.c_str(); }
+const char* ccb_last_error(void) { return LastError(); }
 
 void ccb_params_init(ccb_params* p) {
   if (!p) return;

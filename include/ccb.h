@@ -132,6 +132,18 @@ typedef struct ccb_kernel_stats {
 int ccb_solver_set_profiling(ccb_solver* solver, int32_t enabled);
 int ccb_solver_stats(const ccb_solver* solver, ccb_kernel_stats* stats);
 
+/* ---- device recount -----------------------------------------------------------------------------
+ * Objective f, cluster sizes and G = A*Z of `count` labelings of one graph, computed on the device:
+ * the GPU form of the reference's post-solve recount ObjectiveBitwise (src/cc_pbils_cpu.cpp:25-53,
+ * called from include/cc_cli.hpp:337-343) and of State::Rebuild (src/cc_pbils_cpu.cpp:74-95).
+ * Device pointers: bits (n rows of words_per_row words), labels [count][n] int32, f_out [count];
+ * sizes_out [count][k] and g_out [count][k][n] (int32, cluster-major) may be NULL.  A labeling with a
+ * label outside [0, k) gets f = -1.  Scratch (count * k * ceil(n/32) mask words) is taken from the
+ * stream-ordered allocator for the call.  Asynchronous on `stream`. */
+int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges, int32_t k,
+                           int32_t count, const int32_t* labels, int64_t* f_out, int32_t* sizes_out,
+                           int32_t* g_out, void* stream);
+
 /* ---- host instance generators (the instances of the reference's CLI and of the benchmarks) ----- */
 
 /* Graph::ErdosRenyi (src/cc_graph.cpp:168-177): bits holds n * words_per_row words. Returns edges. */
