@@ -235,3 +235,11 @@ def evaluate_labelings(bits_ptr: int, n: int, words_per_row: int, edges: int, k:
     check(lib().ccb_evaluate_labelings(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr, sizes_ptr,
                                        g_ptr, stream or None))
 
+
+def evaluate_labelings_noalloc(bits_ptr: int, n: int, words_per_row: int, edges: int, k: int, count: int,
+                               labels_ptr: int, f_ptr: int, sizes_ptr: int | None = None, g_ptr: int | None = None,
+                               stream: int = 0) -> None:
+    """ccb_evaluate_labelings_noalloc: the same recount for callers that cannot allocate device memory;
+    its scratch is a fixed 4 MiB device array (count * k * ceil(n / 32) <= 1048576 mask words)."""
+    check(lib().ccb_evaluate_labelings_noalloc(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr,
+                                               sizes_ptr, g_ptr, stream or None))

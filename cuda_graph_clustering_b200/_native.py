@@ -67,6 +67,8 @@ SIGNATURES = {
     "ccb_solver_stats": (C.c_int, [_vp, C.POINTER(CcbKernelStats)]),
     "ccb_evaluate_labelings": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, _vp, _vp,
                                          _vp, _vp, _vp]),
+    "ccb_evaluate_labelings_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32,
+                                                 _vp, _vp, _vp, _vp, _vp]),
     "ccb_generate_erdos_renyi": (C.c_uint64, [_vp, ]),  # argtypes set below (mixed scalar types)
     "ccb_generate_planted": (C.c_uint64, []),
 }

@@ -139,3 +139,80 @@ int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_
 
 }  // extern "C"
 
+// ------------------------------------------------------------------------------------------------
+// Allocation-free recount.
+//
+// Some callers cannot allocate device memory when they call in: a host application whose device
+// memory is already reserved by its own pool allocator (a framework that took the free memory up
+// front, where cudaMalloc fails or fragments that pool), or a latency-critical loop that must not pay
+// cudaMalloc / cudaFree, which can synchronise the whole device.  For them the mask scratch of
+// k_evaluate lives in a fixed array in device memory, loaded with the library: every GPU that loads
+// libccb.so holds these kNoAllocMaskWords words (4 MiB) until the process exits.
+//
+// The array's host-side name is only a stand-in, not a device address, so the entry point looks the
+// address up with cudaGetSymbolAddress once per device (on its first call on that device, with that
+// device current) and passes it to the kernel.  Make that first call before any stream capture.
+// Every call shares the one array and finds the last call's contents there.  k_evaluate writes every
+// mask word it later reads, so nothing needs clearing between calls; but two calls whose kernels
+// overlap on the GPU (different streams, or different host threads) race on the array, so callers
+// must order their calls.
+// ------------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace ccb {
+namespace {
+
+constexpr size_t kNoAllocMaskWords = size_t(1) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) uint32_t g_noalloc_masks[kNoAllocMaskWords];
+
+std::mutex g_noalloc_mutex;
+uint32_t* g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_masks on the current device, looked up once per device.
+cudaError_t NoAllocScratch(uint32_t** out) {
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_address[device] == nullptr) {
+    void* address = nullptr;
+    e = cudaGetSymbolAddress(&address, g_noalloc_masks);
+    if (e != cudaSuccess) return e;
+    g_noalloc_address[device] = static_cast<uint32_t*>(address);
+  }
+  *out = g_noalloc_address[device];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace ccb
+
+extern "C" {
+
+int ccb_evaluate_labelings_noalloc(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                                   int32_t k, int32_t count, const int32_t* labels, int64_t* f_out,
+                                   int32_t* sizes_out, int32_t* g_out, void* stream) {
+  if (const char* why = CheckEvaluateArgs(bits, n, words_per_row, k, count, labels, f_out)) {
+    return Report(CCB_ERR_INVALID, why);
+  }
+  if (count == 0) return Report(CCB_OK, "");
+  const size_t words = (n + 31) / 32;
+  if ((size_t)count * (size_t)k * words > kNoAllocMaskWords) {
+    return Report(CCB_ERR_INVALID,
+                  "ccb_evaluate_labelings_noalloc: count * k * ceil(n / 32) exceeds the 1048576 mask words of "
+                  "its static scratch; split the batch or use ccb_evaluate_labelings");
+  }
+  uint32_t* masks = nullptr;
+  cudaError_t e = NoAllocScratch(&masks);
+  if (e != cudaSuccess) return Report(CCB_ERR_CUDA, cudaGetErrorString(e));
+  k_evaluate<<<count, kEvalThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      bits, (int)n, (int)words, (int)words_per_row, (long long)edges, k, labels, masks, f_out, sizes_out, g_out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return Report(CCB_ERR_CUDA, cudaGetErrorString(e));
+  return Report(CCB_OK, "");
+}
+
+}  // extern "C"
