@@ -1,0 +1,63 @@
+// Instances and launcher of the K <= 8 descent (ccb_descent_small_k.cuh), in a translation unit of their own
+// so that the many template instances compile in parallel with the rest of the library.
+#include <cuda_runtime.h>
+
+#include "ccb_descent_small_k.cuh"
+#include "ccb_plans.h"
+
+namespace ccb {
+namespace {
+
+template <int K, int T, bool S, bool R>
+cudaError_t Go(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_small_k<K, T, S, R>;
+  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel<<<grid, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int K, bool S, bool R>
+cudaError_t ByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool cfg) {
+  switch (threads) {
+    case 128: return Go<K, 128, S, R>(a, grid, smem, st, cfg);
+    case 256: return Go<K, 256, S, R>(a, grid, smem, st, cfg);
+    case 512: return Go<K, 512, S, R>(a, grid, smem, st, cfg);
+    default: return Go<K, 1024, S, R>(a, grid, smem, st, cfg);
+  }
+}
+
+template <int K>
+cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st, bool cfg) {
+  if (p.smem_state && p.smem_rows) return ByThreads<K, true, true>(p.threads, a, grid, p.smem_bytes, st, cfg);
+  if (p.smem_state) return ByThreads<K, true, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
+  return ByThreads<K, false, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
+}
+
+}  // namespace
+
+size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows) {
+  const int kp = PackedLanes(k);
+  size_t b = 0;
+  if (smem_rows) b += ((size_t)n * pitch * 4 + 15) / 16 * 16;
+  if (smem_state) b += (size_t)ld * kp * 2 + ((size_t)ld + 15) / 16 * 16;
+  b += 2 * (size_t)(threads / kWarp) * sizeof(MoveRecord<uint32_t>);
+  return b;
+}
+
+int SmallKLanes(int k) { return PackedLanes(k); }
+
+cudaError_t LaunchDescentSmallK(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st,
+                                bool configure) {
+  switch (p.k) {
+    case 2: return ByPlacement<2>(p, a, grid, st, configure);
+    case 3: return ByPlacement<3>(p, a, grid, st, configure);
+    case 4: return ByPlacement<4>(p, a, grid, st, configure);
+    case 5: return ByPlacement<5>(p, a, grid, st, configure);
+    case 6: return ByPlacement<6>(p, a, grid, st, configure);
+    case 7: return ByPlacement<7>(p, a, grid, st, configure);
+    case 8: return ByPlacement<8>(p, a, grid, st, configure);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace ccb

@@ -138,4 +138,22 @@ __device__ __forceinline__ long long BlockSum(long long v, long long* scratch) {
 
 __device__ __forceinline__ int Bit(const uint32_t* row, int u) { return (row[u >> 5] >> (u & 31)) & 1; }
 
+// Arguments of the descent kernel (passed by value).
+template <typename GainT>
+struct DescentArgs {
+  GraphView gr;
+  PopView<GainT> cur;   // population the tournament draws from (read only)
+  PopView<GainT> next;  // labels and f written here; g used as scratch by the global-state form
+  Control* ctl;
+  int k;
+  int kpad;
+  int ld;
+  int key_bits;         // bit width of n: the vertex field of a move key
+  int population;       // slots in cur (tournament range)
+  int tournament;       // 0: slot s descends from cur[s] (Neighborhood), else tournament size
+  int iteration;
+  uint64_t select_stream;
+};
+
+
 }  // namespace ccb

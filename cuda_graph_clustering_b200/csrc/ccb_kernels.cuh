@@ -96,26 +96,31 @@ __global__ void __launch_bounds__(kThreads) k_rebuild(GraphView gr, PopView<Gain
   for (int c = tid; c < k; c += kThreads) s_sizes[c] = 0;
   __syncthreads();
 
-  // Phase 2: masks of clusters 0 .. k-2 (and sizes of all clusters) by ballots over 32 labels.
-  uint32_t* my_masks = masks + static_cast<size_t>(slot) * k * words;
+  // Phase 2: masks of clusters 0 .. k-2 (and sizes of all clusters) by ballots over 32 labels.  Mask rows
+  // have the graph's pitch; their pad words are never written, which is harmless because the matching
+  // adjacency pad words are zero.
+  const int pitch = gr.pitch;
+  uint32_t* my_masks = masks + static_cast<size_t>(slot) * k * pitch;
   for (int w = warp; w < words; w += kWarps) {
     const int v = w * kWarp + lane;
     const int l = v < n ? labels[v] : -1;
     for (int c = 0; c < k; ++c) {
       const uint32_t m = __ballot_sync(kAllLanes, l == c);
       if (lane == (c % kWarp)) {
-        if (c < k - 1) my_masks[static_cast<size_t>(c) * words + w] = m;
+        if (c < k - 1) my_masks[static_cast<size_t>(c) * pitch + w] = m;
         if (m) atomicAdd(&s_sizes[c], __popc(m));
       }
     }
   }
   __syncthreads();
 
-  // Phase 3: G rows.
+  // Phase 3: one row per thread.  The row streams in as 16-byte vectors (L1 keeps its line while the
+  // thread walks it); every thread of the block reads the same mask vector at the same step, a broadcast.
   GainT* g = cur.g + static_cast<size_t>(slot) * k * ld;
+  const int quads = pitch / 4;
   long long intra_twice = 0;
-  for (int v = warp; v < n; v += kWarps) {
-    const uint32_t* row = gr.bits + static_cast<size_t>(v) * gr.pitch;
+  for (int v = tid; v < n; v += kThreads) {
+    const uint4* row = reinterpret_cast<const uint4*>(gr.bits + static_cast<size_t>(v) * pitch);
     int rest = gr.degrees[v];
     const int own = labels[v];
     int g_own = 0;
@@ -123,55 +128,36 @@ __global__ void __launch_bounds__(kThreads) k_rebuild(GraphView gr, PopView<Gain
       int acc[kChunk];
 #pragma unroll
       for (int i = 0; i < kChunk; ++i) acc[i] = 0;
-      for (int w = lane; w < words; w += kWarp) {
-        const uint32_t a = __ldg(row + w);
+      for (int q = 0; q < quads; ++q) {
+        const uint4 r = __ldg(row + q);
 #pragma unroll
         for (int i = 0; i < kChunk; ++i) {
-          if (c0 + i < k - 1) acc[i] += __popc(a & my_masks[static_cast<size_t>(c0 + i) * words + w]);
+          if (c0 + i < k - 1) {
+            const uint4 m = reinterpret_cast<const uint4*>(my_masks + static_cast<size_t>(c0 + i) * pitch)[q];
+            acc[i] += __popc(r.x & m.x) + __popc(r.y & m.y) + __popc(r.z & m.z) + __popc(r.w & m.w);
+          }
         }
       }
-      int mine = 0;
 #pragma unroll
       for (int i = 0; i < kChunk; ++i) {
         if (c0 + i < k - 1) {
-          const int total = __reduce_add_sync(kAllLanes, static_cast<unsigned>(acc[i]));
-          rest -= total;
-          if (lane == i) mine = total;
-          if (own == c0 + i) g_own = total;
+          g[static_cast<size_t>(c0 + i) * ld + v] = static_cast<GainT>(acc[i]);
+          rest -= acc[i];
+          if (own == c0 + i) g_own = acc[i];
         }
       }
-      if (lane < kChunk && c0 + lane < k - 1) g[static_cast<size_t>(c0 + lane) * ld + v] = static_cast<GainT>(mine);
     }
-    if (lane == 0) {
-      g[static_cast<size_t>(k - 1) * ld + v] = static_cast<GainT>(rest);
-      intra_twice += (own == k - 1) ? rest : g_own;
-    }
+    g[static_cast<size_t>(k - 1) * ld + v] = static_cast<GainT>(rest);
+    intra_twice += (own == k - 1) ? rest : g_own;
   }
   const long long sum = BlockSum<kWarps>(intra_twice, s_sum);
   if (tid == 0) {
-    int sizes_local[kMaxK];
-    for (int c = 0; c < k; ++c) sizes_local[c] = s_sizes[c];
-    cur.f[slot] = gr.edges + PairsInside(sizes_local, k) - sum;
+    long long pairs = 0;
+    for (int c = 0; c < k; ++c) pairs += static_cast<long long>(s_sizes[c]) * (s_sizes[c] - 1) / 2;
+    cur.f[slot] = gr.edges + pairs - sum;
   }
   for (int c = tid; c < k; c += kThreads) cur.sizes[static_cast<size_t>(slot) * kpad + c] = s_sizes[c];
 }
-
-// Arguments of the descent kernel (passed by value).
-template <typename GainT>
-struct DescentArgs {
-  GraphView gr;
-  PopView<GainT> cur;   // population the tournament draws from (read only)
-  PopView<GainT> next;  // labels and f written here; g used as scratch by the global-state form
-  Control* ctl;
-  int k;
-  int kpad;
-  int ld;
-  int key_bits;         // bit width of n: the vertex field of a move key
-  int population;       // slots in cur (tournament range)
-  int tournament;       // 0: slot s descends from cur[s] (Neighborhood), else tournament size
-  int iteration;
-  uint64_t select_stream;
-};
 
 // Steepest descent of one slot per block until no strictly improving single-vertex move remains.
 //

@@ -1,0 +1,26 @@
+// Launch plans shared between the solver and the separately compiled descent instances.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "ccb_device.cuh"
+
+namespace ccb {
+
+// Descent specialised for 2 <= k <= 8 on the narrow path (ccb_descent_small_k.cuh).
+struct SmallKPlan {
+  int k = 0;
+  int threads = 256;
+  bool smem_state = false;  // packed G + labels in shared memory (else the slot's rows of `next`)
+  bool smem_rows = false;   // whole bitset in shared memory
+  size_t smem_bytes = 0;
+};
+
+size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows);
+int SmallKLanes(int k);
+cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
+                                cudaStream_t stream, bool configure);
+
+}  // namespace ccb

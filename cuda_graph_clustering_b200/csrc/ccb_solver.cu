@@ -21,6 +21,7 @@
 #include "ccb.h"
 #include "ccb_error.h"
 #include "ccb_kernels.cuh"
+#include "ccb_plans.h"
 
 namespace ccb {
 
@@ -212,7 +213,16 @@ struct Plan {
   int threads = 512;
   size_t smem_bytes = 0;
   int key_bits = 0;
+  bool small_k = false;     // the packed K <= 8 descent (ccb_descent_small_k.cuh)
+  SmallKPlan sk;
 };
+
+int SmallKThreads(int n) {
+  if (n <= 256) return 128;
+  if (n <= 1024) return 256;
+  if (n <= 4096) return 512;
+  return 1024;
+}
 
 int DescentThreads(int n, bool wide) {
   if (wide) return 1024;
@@ -254,6 +264,19 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
     p.smem_rows = DescentSmem(with_rows, n, pitch, k, ld, kpad) <= limit;
   }
   p.smem_bytes = DescentSmem(p, n, pitch, k, ld, kpad);
+  if (!p.wide && k >= 2 && k <= 8 && ls_kernel == CCB_LS_AUTO) {
+    SmallKPlan& sk = p.sk;
+    sk.k = k;
+    sk.threads = SmallKThreads(n);
+    sk.smem_state = SmallKSmem(k, n, pitch, ld, sk.threads, true, false) <= limit;
+    sk.smem_rows = sk.smem_state && SmallKSmem(k, n, pitch, ld, sk.threads, true, true) <= limit;
+    sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, sk.smem_rows);
+    p.small_k = true;
+    p.smem_state = sk.smem_state;
+    p.smem_rows = sk.smem_rows;
+    p.threads = sk.threads;
+    p.smem_bytes = sk.smem_bytes;
+  }
   return p;
 }
 
@@ -296,6 +319,11 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 }
 
 const char* KernelName(const Plan& p) {
+  if (p.small_k) {
+    if (p.smem_state) return p.smem_rows ? "packed k <= 8, shared memory, bitset in shared memory"
+                                         : "packed k <= 8, shared memory";
+    return "packed k <= 8, global memory";
+  }
   if (p.wide) return "generic wide (int32 G), global memory";
   if (p.smem_state) return p.smem_rows ? "generic, shared memory, bitset in shared memory" : "generic, shared memory";
   return p.smem_rows ? "generic, global memory, bitset in shared memory" : "generic, global memory";
@@ -437,8 +465,9 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   const size_t labels = (size_t)pop * s->ld;
   const size_t gains = labels * k;
   const size_t gb = s->GainBytes();
-  size_t bytes = 2 * labels + gains * gb * (s->plan.smem_state ? 1 : 2) + (size_t)pop * s->kpad * 4 + 2 * pop * 8 +
-                 (size_t)pop * k * g->words * 4 + 2 * (size_t)pop * 4 + s->ld + sizeof(Control);
+  const size_t next_lanes = s->plan.smem_state ? 0 : (s->plan.small_k ? std::max(k, SmallKLanes(k)) : k);
+  size_t bytes = 2 * labels + gains * gb + labels * next_lanes * gb + (size_t)pop * s->kpad * 4 + 2 * pop * 8 +
+                 (size_t)pop * k * g->pitch * 4 + 2 * (size_t)pop * 4 + s->ld + sizeof(Control);
   size_t free_b = 0, total_b = 0;
   CCB_CUDA(cudaMemGetInfo(&free_b, &total_b));
   if (bytes > free_b) {
@@ -451,14 +480,16 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->Alloc(cg, gains * gb);
   s->cur_g = cg;
   if (!s->plan.smem_state) {
+    // the global-state descents work in the slot's rows of next: cluster-major G, or packed vectors
+    const size_t lanes = s->plan.small_k ? std::max(k, SmallKLanes(k)) : k;
     uint8_t* ng = nullptr;
-    s->Alloc(ng, gains * gb);
+    s->Alloc(ng, labels * lanes * gb);
     s->next_g = ng;
   }
   s->Alloc(s->cur_sizes, (size_t)pop * s->kpad);
   s->Alloc(s->cur_f, pop);
   s->Alloc(s->next_f, pop);
-  s->Alloc(s->masks, (size_t)pop * k * g->words);
+  s->Alloc(s->masks, (size_t)pop * k * g->pitch);
   s->Alloc(s->src_map, pop);
   s->Alloc(s->order, pop);
   s->Alloc(s->record_lab, s->ld);
@@ -471,7 +502,9 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   CCB_CUDA(cudaEventCreateWithFlags(&s->poll_event[1], cudaEventDisableTiming));
 
   // Shared-memory opt-in for the descent instance of this plan.
-  if (s->plan.wide) {
+  if (s->plan.small_k) {
+    CCB_CUDA(LaunchDescentSmallK(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
+  } else if (s->plan.wide) {
     LaunchDescent<int32_t>(s->plan, DescentArgs<int32_t>{}, 0, nullptr, true);
   } else {
     LaunchDescent<int16_t>(s->plan, DescentArgs<int16_t>{}, 0, nullptr, true);
@@ -522,6 +555,14 @@ void LaunchDescentStep(ccb_solver& s, int grid, int population, int tournament, 
   a.tournament = tournament;
   a.iteration = iteration;
   a.select_stream = stream;
+  if constexpr (std::is_same_v<GainT, int16_t>) {
+    if (s.plan.small_k) {
+      cudaError_t e = cudaSuccess;
+      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentSmallK(s.plan.sk, a, grid, st, false); });
+      CCB_CUDA(e);
+      return;
+    }
+  }
   s.timer.Time(kCatDescent, st, [&] { LaunchDescent<GainT>(s.plan, a, grid, st, false); });
   CCB_CUDA(cudaGetLastError());
 }
