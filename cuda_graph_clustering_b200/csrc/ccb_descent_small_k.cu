@@ -2,6 +2,7 @@
 // so that the many template instances compile in parallel with the rest of the library.
 #include <cuda_runtime.h>
 
+#include "ccb_descent_registers.cuh"
 #include "ccb_descent_small_k.cuh"
 #include "ccb_plans.h"
 
@@ -26,8 +27,31 @@ cudaError_t ByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size
   }
 }
 
+template <int K, int T, bool R>
+cudaError_t GoRegisters(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_registers<K, T, R>;
+  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel<<<grid, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int K, bool R>
+cudaError_t RegistersByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st,
+                               bool cfg) {
+  switch (threads) {
+    case 128: return GoRegisters<K, 128, R>(a, grid, smem, st, cfg);
+    case 256: return GoRegisters<K, 256, R>(a, grid, smem, st, cfg);
+    case 512: return GoRegisters<K, 512, R>(a, grid, smem, st, cfg);
+    default: return GoRegisters<K, 1024, R>(a, grid, smem, st, cfg);
+  }
+}
+
 template <int K>
 cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st, bool cfg) {
+  if (p.registers) {
+    return p.smem_rows ? RegistersByThreads<K, true>(p.threads, a, grid, p.smem_bytes, st, cfg)
+                       : RegistersByThreads<K, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
+  }
   if (p.smem_state && p.smem_rows) return ByThreads<K, true, true>(p.threads, a, grid, p.smem_bytes, st, cfg);
   if (p.smem_state) return ByThreads<K, true, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
   return ByThreads<K, false, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
@@ -45,6 +69,12 @@ size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state,
 }
 
 int SmallKLanes(int k) { return PackedLanes(k); }
+
+size_t RegistersSmem(int n, int pitch, bool smem_rows) {
+  return smem_rows ? ((size_t)n * pitch * 4 + 15) / 16 * 16 : 0;
+}
+
+int RegistersMaxVertices(int threads) { return kRegVerticesPerThread * threads; }
 
 cudaError_t LaunchDescentSmallK(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st,
                                 bool configure) {

@@ -267,10 +267,19 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
   if (!p.wide && k >= 2 && k <= 8 && ls_kernel == CCB_LS_AUTO) {
     SmallKPlan& sk = p.sk;
     sk.k = k;
-    sk.threads = SmallKThreads(n);
-    sk.smem_state = SmallKSmem(k, n, pitch, ld, sk.threads, true, false) <= limit;
-    sk.smem_rows = sk.smem_state && SmallKSmem(k, n, pitch, ld, sk.threads, true, true) <= limit;
-    sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, sk.smem_rows);
+    if (n <= RegistersMaxVertices(1024)) {
+      sk.registers = true;
+      sk.smem_state = true;  // nothing of the state lives in global memory
+      sk.threads = 128;
+      while (RegistersMaxVertices(sk.threads) < n) sk.threads *= 2;
+      sk.smem_rows = RegistersSmem(n, pitch, true) <= limit;
+      sk.smem_bytes = RegistersSmem(n, pitch, sk.smem_rows);
+    } else {
+      sk.threads = SmallKThreads(n);
+      sk.smem_state = SmallKSmem(k, n, pitch, ld, sk.threads, true, false) <= limit;
+      sk.smem_rows = sk.smem_state && SmallKSmem(k, n, pitch, ld, sk.threads, true, true) <= limit;
+      sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, sk.smem_rows);
+    }
     p.small_k = true;
     p.smem_state = sk.smem_state;
     p.smem_rows = sk.smem_rows;
@@ -320,6 +329,8 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 
 const char* KernelName(const Plan& p) {
   if (p.small_k) {
+    if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
+                                           : "packed k <= 8, registers";
     if (p.smem_state) return p.smem_rows ? "packed k <= 8, shared memory, bitset in shared memory"
                                          : "packed k <= 8, shared memory";
     return "packed k <= 8, global memory";
