@@ -1,68 +1,32 @@
-// Steepest descent with the whole slot state in registers: compile-time K <= 8, four vertices per thread
-// (u = tid + j * T, j < 4), n <= 4 * T <= 4096.  Same trajectory as k_descent and the reference's
-// BestMove/ApplyMove (src/cc_pbils_cpu.cpp:99-139).
+// Steepest descent with the slot state in registers as move keys: compile-time K <= 8, V vertices per thread
+// (u = tid + j * T, j < V), n <= V * T.  Same trajectory as k_descent and the reference's BestMove/ApplyMove
+// (src/cc_pbils_cpu.cpp:99-139).
 //
-// Per owned vertex a thread keeps
-//   g[j]    the K counters G_c(u) in 16-bit lanes of one 4/8/16-byte vector, the own cluster's lane with its
-//           top bit set (G_a + 2^15, never carries: G <= n - 1 < 2^15);
-//   lab[j]  the label a(u);
-//   hown[j] h_a(u) = size_a - 2 G_a(u), kept up to date move by move;
-// and every thread keeps off[c] = 16 size_c + c.  The key of moving u to c is off[c] - 32 G_c(u) =
-// 16 h_c(u) + c; read through a sign-extending unpack, the own lane's key carries a +2^20 penalty, which for
-// n <= 21844 exceeds the spread of all keys, so the best foreign target is a plain minimum over the lanes
-// (smallest h, then lowest cluster: the reference's rule).  A move (v: from -> to) changes, for every u,
-//   h_from += 2 adj - 1,  h_to += 1 - 2 adj      (adj = u is a neighbour of v),
-// and for neighbours G_from -= 1, G_to += 1 (one packed add).  The moved vertex's own lane moves from `from`
-// to `to` and its h_own becomes its old h_to (the uniform update then adds the size change).
+// For each owned vertex u a thread keeps K 32-bit keys
+//     key_c(u) = 16 h_c(u) + c  (+ 2^20 for c = the label of u),   h_c(u) = size_c - 2 G_c(u),
+// so the key of moving u to c orders candidates by h, then by the lower cluster: the reference's rule
+// (MoveDelta, cc_math.hpp:75-77: the gain of a -> c is h_c - h_a + 1).  The 2^20 penalty exceeds the
+// spread 48 n + 15 of unpenalised keys for n <= 21844, so over the K lanes the minimum is the best foreign
+// target and the maximum is the vertex's own cluster: no label, no G, no per-cluster offset is stored.
+//
+// A move (v: from -> to) shifts, for every vertex u, key_from by +16 if u is a neighbour of v and -16
+// otherwise (size_from - 1, and G_from - 1 for neighbours), and key_to by the opposite amount; with the
+// per-move coefficients coef_c = [c = from] - [c = to] that is one multiply-add per lane, folded into the
+// scan of the next move.  The moved vertex itself (not its own neighbour) also moves its penalty from lane
+// `from` to lane `to`.
 #pragma once
 
 #include <cstdint>
 
-#include "ccb_descent_small_k.cuh"
 #include "ccb_device.cuh"
 
 namespace ccb {
 
-constexpr int kRegVerticesPerThread = 4;
-constexpr int kRegMaxVertices = 21844;  // limit of the own-lane penalty (48 n < 2^20 - 15)
+constexpr int kRegPenalty = 1 << 20;
+constexpr int kRegMaxVertices = 21844;  // 48 n + 15 < 2^20
 
-// Key contribution 32 * lane c, read as a signed 16-bit value (so the own lane comes out negative).
-template <int KP, int C>
-__device__ __forceinline__ int Scaled32(const typename PackedGains<KP>::Vec& v) {
-  const uint32_t word = PackedGains<KP>::Word(v, C / 2);
-  if constexpr (C & 1) {
-    return (static_cast<int>(word) >> 16) * 32;
-  } else {
-    return static_cast<int>(word << 16) >> 11;
-  }
-}
-
-template <int K, int KP, int C>
-struct LaneMin {
-  __device__ __forceinline__ static int Run(const typename PackedGains<KP>::Vec& v, const int* off, int acc) {
-    acc = min(acc, off[C] - Scaled32<KP, C>(v));
-    return LaneMin<K, KP, C + 1>::Run(v, off, acc);
-  }
-};
-template <int K, int KP>
-struct LaneMin<K, KP, K> {
-  __device__ __forceinline__ static int Run(const typename PackedGains<KP>::Vec&, const int*, int acc) { return acc; }
-};
-
-template <int KP>
-__device__ __forceinline__ void AddLane(typename PackedGains<KP>::Vec& v, int lane, uint32_t amount) {
-  uint32_t d[PackedGains<KP>::kWords];
-#pragma unroll
-  for (int i = 0; i < PackedGains<KP>::kWords; ++i) d[i] = (lane >> 1) == i ? (amount << (16 * (lane & 1))) : 0u;
-  PackedGains<KP>::Add(v, d);
-}
-
-template <int K, int T, bool kSmemRows>
+template <int K, int T, int V, bool kSmemRows>
 __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t> a) {
-  constexpr int KP = PackedLanes(K);
-  constexpr int V = kRegVerticesPerThread;
-  using P = PackedGains<KP>;
-  using Vec = typename P::Vec;
   constexpr int kWarps = T / kWarp;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
@@ -97,49 +61,27 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
   if (s_stop) return;
   const int w = s_winner;
 
-  int off[K];
-  {
-    const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
-#pragma unroll
-    for (int c = 0; c < K; ++c) off[c] = 16 * sizes[c] + c;
-  }
-  Vec g[V];
-  int lab[V];
-  int hown[V];
-  int ucode[V];  // (2^B << B) | u: adding gain << B gives the move key
+  int key[V][K];
+  int ucode[V];  // (2^B << B) | u: adding gain << B gives the block-wide move key
   unsigned valid = 0;
   {
     const int16_t* g_src = a.cur.g + static_cast<size_t>(w) * K * ld;
     const uint8_t* l_src = a.cur.labels + static_cast<size_t>(w) * ld;
+    const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+    int s16[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) s16[c] = 16 * sizes[c] + c;
 #pragma unroll
     for (int j = 0; j < V; ++j) {
       const int u = tid + j * T;
-      uint32_t words[P::kWords];
+      const bool ok = u < n;
+      valid |= ok ? (1u << j) : 0u;
+      const int own = ok ? l_src[u] : 0;
 #pragma unroll
-      for (int i = 0; i < P::kWords; ++i) words[i] = 0;
-      int own = 0, g_own = 0;
-      if (u < n) {
-        valid |= 1u << j;
-        own = l_src[u];
-#pragma unroll
-        for (int c = 0; c < K; ++c) {
-          const int gc = g_src[static_cast<size_t>(c) * ld + u];
-          words[c / 2] |= static_cast<uint32_t>(gc + (c == own ? 0x8000 : 0)) << (16 * (c & 1));
-          if (c == own) g_own = gc;
-        }
+      for (int c = 0; c < K; ++c) {
+        const int gc = ok ? g_src[static_cast<size_t>(c) * ld + u] : 0;
+        key[j][c] = s16[c] - 32 * gc + (c == own ? kRegPenalty : 0);
       }
-      if constexpr (KP == 2) {
-        g[j] = words[0];
-      } else if constexpr (KP == 4) {
-        g[j] = make_uint2(words[0], words[1]);
-      } else {
-        g[j] = make_uint4(words[0], words[1], words[2], words[3]);
-      }
-      lab[j] = own;
-      int s_own = 0;
-#pragma unroll
-      for (int c = 0; c < K; ++c) s_own = (c == own) ? (off[c] >> 4) : s_own;
-      hown[j] = s_own - 2 * g_own;
       ucode[j] = ((1 << bits) << bits) | u;
     }
   }
@@ -148,62 +90,55 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
 
   unsigned long long applied = 0;
   int parity = 0;
-  bool pending = false;  // a move whose neighbour update is still to be folded in
-  int from = 0, to = 0;
-  const uint32_t* prev_row = rows;
-  uint32_t delta[P::kWords];
+  bool pending = false;  // a move still to be folded into the keys
+  int coef[K];           // [c = from] - [c = to] of that move
 #pragma unroll
-  for (int i = 0; i < P::kWords; ++i) delta[i] = 0;
+  for (int c = 0; c < K; ++c) coef[c] = 0;
+  const uint32_t* prev_row = rows;
   const uint32_t lane_bit = 1u << lane;
 
   while (true) {
-    // Fold the previous move into the owned vertices, then score them.
     uint32_t rw[V];
 #pragma unroll
     for (int j = 0; j < V; ++j) rw[j] = (pending && ((valid >> j) & 1)) ? prev_row[(tid + j * T) >> 5] : 0u;
-    int kb[V];
-    uint32_t key[V];
     uint32_t best = KeyTraits<uint32_t>::kNone;
-#pragma unroll
-    for (int j = 0; j < V; ++j) {
-      const bool adj = (rw[j] & lane_bit) != 0;
-      if (adj) P::Add(g[j], delta);
-      if (pending) {
-        const int d = adj ? 1 : -1;  // h_from += 2 adj - 1, h_to -= 2 adj - 1
-        hown[j] += (lab[j] == from ? d : 0) - (lab[j] == to ? d : 0);
-      }
-      kb[j] = LaneMin<K, KP, 0>::Run(g[j], off, 0x7fffffff);
-      const int gain = (kb[j] >> 4) - hown[j] + 1;
-      key[j] = (gain < 0 && ((valid >> j) & 1)) ? static_cast<uint32_t>(gain * (1 << bits) + ucode[j])
-                                                : KeyTraits<uint32_t>::kNone;
-      best = min(best, key[j]);
-    }
     uint32_t payload = 0;
 #pragma unroll
-    for (int j = V - 1; j >= 0; --j) {
-      if (key[j] == best) payload = static_cast<uint32_t>(lab[j]) | (static_cast<uint32_t>(kb[j] & 15) << 8);
+    for (int j = 0; j < V; ++j) {
+      const int d = (rw[j] & lane_bit) ? 16 : -16;
+#pragma unroll
+      for (int c = 0; c < K; ++c) key[j][c] += coef[c] * d;
+      int kmin = key[j][0], kmax = key[j][0];
+#pragma unroll
+      for (int c = 1; c < K; ++c) {
+        kmin = min(kmin, key[j][c]);
+        kmax = max(kmax, key[j][c]);
+      }
+      const int gain = (kmin >> 4) - (kmax >> 4) + (kRegPenalty >> 4) + 1;
+      const uint32_t mk = (gain < 0 && ((valid >> j) & 1)) ? static_cast<uint32_t>(gain * (1 << bits) + ucode[j])
+                                                           : KeyTraits<uint32_t>::kNone;
+      if (mk < best) {
+        best = mk;
+        payload = static_cast<uint32_t>(kmax & 15) | (static_cast<uint32_t>(kmin & 15) << 8);
+      }
     }
     const MoveRecord<uint32_t> m = BlockArgMin<uint32_t, kWarps>(best, payload, s_records + parity * kWarps);
     if (m.key == KeyTraits<uint32_t>::kNone) break;
     parity ^= 1;
 
     const int v = MoveVertex(m.key, bits);
-    from = static_cast<int>(m.payload & 0xff);
-    to = static_cast<int>(m.payload >> 8);
+    const int from = static_cast<int>(m.payload & 0xff);
+    const int to = static_cast<int>(m.payload >> 8);
 #pragma unroll
-    for (int c = 0; c < K; ++c) off[c] += (c == to ? 16 : 0) - (c == from ? 16 : 0);
+    for (int c = 0; c < K; ++c) coef[c] = (c == from ? 1 : 0) - (c == to ? 1 : 0);
+    if (v % T == tid) {
+      const int jv = v / T;
 #pragma unroll
-    for (int i = 0; i < P::kWords; ++i) {
-      delta[i] = ((to >> 1) == i ? (1u << (16 * (to & 1))) : 0u) - ((from >> 1) == i ? (1u << (16 * (from & 1))) : 0u);
-    }
+      for (int j = 0; j < V; ++j) {
+        if (j == jv) {
 #pragma unroll
-    for (int j = 0; j < V; ++j) {
-      if (v == tid + j * T) {
-        // the moved vertex: own lane from -> to, h_own = its old h_to (the size change is added above)
-        AddLane<KP>(g[j], from, 0xFFFF8000u);  // - 2^15 in lane `from` (its top bit is set: no borrow)
-        AddLane<KP>(g[j], to, 0x8000u);
-        hown[j] = kb[j] >> 4;
-        lab[j] = to;
+          for (int c = 0; c < K; ++c) key[j][c] -= coef[c] * kRegPenalty;
+        }
       }
     }
     prev_row = rows + static_cast<size_t>(v) * a.gr.pitch;
@@ -219,7 +154,12 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
   uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
 #pragma unroll
   for (int j = 0; j < V; ++j) {
-    if ((valid >> j) & 1) dst[tid + j * T] = static_cast<uint8_t>(lab[j]);
+    if ((valid >> j) & 1) {
+      int kmax = key[j][0];
+#pragma unroll
+      for (int c = 1; c < K; ++c) kmax = max(kmax, key[j][c]);
+      dst[tid + j * T] = static_cast<uint8_t>(kmax & 15);
+    }
   }
   if (tid == 0) {
     a.next.f[slot] = objective;

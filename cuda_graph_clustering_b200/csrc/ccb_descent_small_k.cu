@@ -27,30 +27,37 @@ cudaError_t ByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size
   }
 }
 
-template <int K, int T, bool R>
+template <int K, int T, int V, bool R>
 cudaError_t GoRegisters(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
-  auto kernel = k_descent_registers<K, T, R>;
+  auto kernel = k_descent_registers<K, T, V, R>;
   if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int K, bool R>
-cudaError_t RegistersByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st,
-                               bool cfg) {
+cudaError_t RegistersByShape(int threads, int vpt, const DescentArgs<int16_t>& a, int grid, size_t smem,
+                             cudaStream_t st, bool cfg) {
+  if (vpt == 8) {
+    switch (threads) {
+      case 128: return GoRegisters<K, 128, 8, R>(a, grid, smem, st, cfg);
+      case 256: return GoRegisters<K, 256, 8, R>(a, grid, smem, st, cfg);
+      default: return GoRegisters<K, 512, 8, R>(a, grid, smem, st, cfg);
+    }
+  }
   switch (threads) {
-    case 128: return GoRegisters<K, 128, R>(a, grid, smem, st, cfg);
-    case 256: return GoRegisters<K, 256, R>(a, grid, smem, st, cfg);
-    case 512: return GoRegisters<K, 512, R>(a, grid, smem, st, cfg);
-    default: return GoRegisters<K, 1024, R>(a, grid, smem, st, cfg);
+    case 128: return GoRegisters<K, 128, 4, R>(a, grid, smem, st, cfg);
+    case 256: return GoRegisters<K, 256, 4, R>(a, grid, smem, st, cfg);
+    case 512: return GoRegisters<K, 512, 4, R>(a, grid, smem, st, cfg);
+    default: return GoRegisters<K, 1024, 4, R>(a, grid, smem, st, cfg);
   }
 }
 
 template <int K>
 cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st, bool cfg) {
   if (p.registers) {
-    return p.smem_rows ? RegistersByThreads<K, true>(p.threads, a, grid, p.smem_bytes, st, cfg)
-                       : RegistersByThreads<K, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
+    return p.smem_rows ? RegistersByShape<K, true>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg)
+                       : RegistersByShape<K, false>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg);
   }
   if (p.smem_state && p.smem_rows) return ByThreads<K, true, true>(p.threads, a, grid, p.smem_bytes, st, cfg);
   if (p.smem_state) return ByThreads<K, true, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
@@ -74,7 +81,10 @@ size_t RegistersSmem(int n, int pitch, bool smem_rows) {
   return smem_rows ? ((size_t)n * pitch * 4 + 15) / 16 * 16 : 0;
 }
 
-int RegistersMaxVertices(int threads) { return kRegVerticesPerThread * threads; }
+bool RegistersShapeBuilt(int threads, int vpt) {
+  return (vpt == 8 && (threads == 128 || threads == 256 || threads == 512)) ||
+         (vpt == 4 && (threads == 128 || threads == 256 || threads == 512 || threads == 1024));
+}
 
 cudaError_t LaunchDescentSmallK(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st,
                                 bool configure) {

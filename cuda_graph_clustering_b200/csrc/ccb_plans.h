@@ -13,7 +13,8 @@ namespace ccb {
 struct SmallKPlan {
   int k = 0;
   int threads = 256;
-  bool registers = false;   // whole state in registers (ccb_descent_registers.cuh), n <= 4 * threads
+  bool registers = false;   // whole state in registers (ccb_descent_registers.cuh), n <= vpt * threads
+  int vpt = 4;              // vertices per thread of the register form (4 or 8)
   bool smem_state = false;  // packed G + labels in shared memory (else the slot's rows of `next`)
   bool smem_rows = false;   // whole bitset in shared memory
   size_t smem_bytes = 0;
@@ -22,7 +23,7 @@ struct SmallKPlan {
 size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows);
 int SmallKLanes(int k);
 size_t RegistersSmem(int n, int pitch, bool smem_rows);
-int RegistersMaxVertices(int threads);
+bool RegistersShapeBuilt(int threads, int vpt);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);
 

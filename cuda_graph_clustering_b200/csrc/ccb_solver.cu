@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -217,6 +218,22 @@ struct Plan {
   SmallKPlan sk;
 };
 
+// Threads and vertices per thread of the register descent: the smallest block that covers n with 4
+// vertices per thread (measured on the plain configuration, n = 1000, k = 5: 256 x 4 beats 128 x 8 by 10%
+// and 512 x 4 by 50%); CCB_REG_SHAPE=T,V overrides it for tuning sweeps.
+void RegisterShape(int n, int* threads, int* vpt) {
+  *vpt = 4;
+  *threads = 128;
+  while (*threads * *vpt < n) *threads *= 2;
+  if (const char* env = std::getenv("CCB_REG_SHAPE")) {
+    int t = 0, v = 0;
+    if (std::sscanf(env, "%d,%d", &t, &v) == 2 && RegistersShapeBuilt(t, v) && t * v >= n) {
+      *threads = t;
+      *vpt = v;
+    }
+  }
+}
+
 int SmallKThreads(int n) {
   if (n <= 256) return 128;
   if (n <= 1024) return 256;
@@ -267,11 +284,10 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
   if (!p.wide && k >= 2 && k <= 8 && ls_kernel == CCB_LS_AUTO) {
     SmallKPlan& sk = p.sk;
     sk.k = k;
-    if (n <= RegistersMaxVertices(1024)) {
+    if (n <= 4096) {
       sk.registers = true;
       sk.smem_state = true;  // nothing of the state lives in global memory
-      sk.threads = 128;
-      while (RegistersMaxVertices(sk.threads) < n) sk.threads *= 2;
+      RegisterShape(n, &sk.threads, &sk.vpt);
       sk.smem_rows = RegistersSmem(n, pitch, true) <= limit;
       sk.smem_bytes = RegistersSmem(n, pitch, sk.smem_rows);
     } else {
