@@ -35,6 +35,11 @@ sys.path.insert(0, REPO)
 PLAIN = dict(n=1000, density=0.5, graph_seed=1, k=5, population=128, tournament=5, perturbation=0.4, gww=0.1,
              iterations=100, early_stop=100, seed=1)
 PLAIN_OBJECTIVE = {1: 234911}  # seed -> objective of the CPU oracle (and the reference binary)
+# The large plain configuration of the hot-path roofline target: G(32000, 0.33) from graph seed 7, k=8,
+# pop 128; a step is a short solve (3 iterations) because one iteration costs ~10^4 moves per slot.
+NORTH = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournament=5, perturbation=0.4, gww=0.1,
+             iterations=3, early_stop=100, seed=1)
+WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "north": (NORTH, {})}
 
 
 def parse():
@@ -43,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["plain"], default="plain")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -192,7 +197,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    cfg = dict(PLAIN)
+    cfg, objectives = WORKLOADS[args.workload]
+    cfg = dict(cfg)
     seed = cfg["seed"] + rank
     graph = ccb.Graph.ErdosRenyi(cfg["n"], cfg["density"], cfg["graph_seed"])
     params = ccb.PbilsParams(k=cfg["k"], population=cfg["population"], tournament=cfg["tournament"],
@@ -203,7 +209,7 @@ def main():
     dg = ccb.DeviceGraph(graph, stream=sh)
     solver = ccb.Solver(dg, params)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    expected = PLAIN_OBJECTIVE.get(seed)
+    expected = objectives.get(seed)
 
     def barrier():
         if dist is not None:
@@ -281,19 +287,22 @@ def main():
         per_launch = moves_per_launch * per_move + pop * (k * ld * 2 + 2 * ld)
         peak, peak_kind = measured_peak_hbm()
         achieved = per_launch / (descent_ms * 1e-3) / 1e9
-        traffic = profiled_traffic("k_descent_plain_n1000")
+        traffic = profiled_traffic(f"k_descent_{args.workload}")
         value = iters_all / (total_ms_all * 1e-3)
         cpu = None
         if not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
-            t, f, threads = reference_cpu_run(cfg, 20)
-            cpu = {"value": 20 / t, "unit": "iter/s", "cores": threads, "kind": "reference",
-                   "sample": "20 of the 100 iterations of the same instance and seed, --threads 0"}
+            sample = 20 if args.workload == "plain" else 1
+            t, f, threads = reference_cpu_run(cfg, sample)
+            cpu = {"value": sample / t, "unit": "iter/s", "cores": threads, "kind": "reference",
+                   "sample": f"{sample} of the {cfg['iterations']} iterations of the same instance and seed, "
+                             "--threads 0"}
         line = {
             "metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
-            "config": {"workload": "plain PBILS: ER(n=1000, p=0.5, graph seed 1), k=5, pop=128, tournament 5, "
-                                   "perturb 0.4, gww 0.1, 100 iterations (early stop off), seed 1 + rank",
+            "config": {"workload": f"{args.workload} PBILS: ER(n={n}, p={cfg['density']}, graph seed "
+                                   f"{cfg['graph_seed']}), k={k}, pop={pop}, tournament 5, perturb 0.4, gww 0.1, "
+                                   f"{cfg['iterations']} iterations (early stop off), seed {cfg['seed']} + rank",
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "kernel_plan": solver.describe()},
             "ls_moves_per_s": moves_all / (total_ms_all * 1e-3),

@@ -3,28 +3,18 @@
 #include <cuda_runtime.h>
 
 #include "ccb_descent_registers.cuh"
-#include "ccb_descent_small_k.cuh"
+#include "ccb_descent_stream.cuh"
 #include "ccb_plans.h"
 
 namespace ccb {
 namespace {
 
-template <int K, int T, bool S, bool R>
-cudaError_t Go(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
-  auto kernel = k_descent_small_k<K, T, S, R>;
+template <int K, int T, bool S>
+cudaError_t GoStream(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_stream<K, T, S>;
   if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
-}
-
-template <int K, bool S, bool R>
-cudaError_t ByThreads(int threads, const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool cfg) {
-  switch (threads) {
-    case 128: return Go<K, 128, S, R>(a, grid, smem, st, cfg);
-    case 256: return Go<K, 256, S, R>(a, grid, smem, st, cfg);
-    case 512: return Go<K, 512, S, R>(a, grid, smem, st, cfg);
-    default: return Go<K, 1024, S, R>(a, grid, smem, st, cfg);
-  }
 }
 
 template <int K, int T, int V, bool R>
@@ -59,20 +49,21 @@ cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int 
     return p.smem_rows ? RegistersByShape<K, true>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg)
                        : RegistersByShape<K, false>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg);
   }
-  if (p.smem_state && p.smem_rows) return ByThreads<K, true, true>(p.threads, a, grid, p.smem_bytes, st, cfg);
-  if (p.smem_state) return ByThreads<K, true, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
-  return ByThreads<K, false, false>(p.threads, a, grid, p.smem_bytes, st, cfg);
+  if (p.threads == 512) {
+    return p.smem_state ? GoStream<K, 512, true>(a, grid, p.smem_bytes, st, cfg)
+                        : GoStream<K, 512, false>(a, grid, p.smem_bytes, st, cfg);
+  }
+  return p.smem_state ? GoStream<K, 1024, true>(a, grid, p.smem_bytes, st, cfg)
+                      : GoStream<K, 1024, false>(a, grid, p.smem_bytes, st, cfg);
 }
 
 }  // namespace
 
 size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows) {
-  const int kp = PackedLanes(k);
-  size_t b = 0;
-  if (smem_rows) b += ((size_t)n * pitch * 4 + 15) / 16 * 16;
-  if (smem_state) b += (size_t)ld * kp * 2 + ((size_t)ld + 15) / 16 * 16;
-  b += 2 * (size_t)(threads / kWarp) * sizeof(MoveRecord<uint32_t>);
-  return b;
+  (void)pitch;
+  (void)threads;
+  (void)smem_rows;
+  return smem_state ? (size_t)ld * PackedLanes(k) * 2 : 0;
 }
 
 int SmallKLanes(int k) { return PackedLanes(k); }

@@ -234,12 +234,6 @@ void RegisterShape(int n, int* threads, int* vpt) {
   }
 }
 
-int SmallKThreads(int n) {
-  if (n <= 256) return 128;
-  if (n <= 1024) return 256;
-  if (n <= 4096) return 512;
-  return 1024;
-}
 
 int DescentThreads(int n, bool wide) {
   if (wide) return 1024;
@@ -291,10 +285,10 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
       sk.smem_rows = RegistersSmem(n, pitch, true) <= limit;
       sk.smem_bytes = RegistersSmem(n, pitch, sk.smem_rows);
     } else {
-      sk.threads = SmallKThreads(n);
+      sk.threads = 1024;
       sk.smem_state = SmallKSmem(k, n, pitch, ld, sk.threads, true, false) <= limit;
-      sk.smem_rows = sk.smem_state && SmallKSmem(k, n, pitch, ld, sk.threads, true, true) <= limit;
-      sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, sk.smem_rows);
+      sk.smem_rows = false;
+      sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, false);
     }
     p.small_k = true;
     p.smem_state = sk.smem_state;
@@ -347,9 +341,7 @@ const char* KernelName(const Plan& p) {
   if (p.small_k) {
     if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
                                            : "packed k <= 8, registers";
-    if (p.smem_state) return p.smem_rows ? "packed k <= 8, shared memory, bitset in shared memory"
-                                         : "packed k <= 8, shared memory";
-    return "packed k <= 8, global memory";
+    return p.smem_state ? "packed k <= 8, streamed from shared memory" : "packed k <= 8, streamed from L2";
   }
   if (p.wide) return "generic wide (int32 G), global memory";
   if (p.smem_state) return p.smem_rows ? "generic, shared memory, bitset in shared memory" : "generic, shared memory";

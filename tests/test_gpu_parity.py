@@ -216,3 +216,14 @@ def test_shared_kernel_rejects_oversized_state(ccb, oracle, cuda_device):
     with pytest.raises(RuntimeError) as e:
         ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, k=16, population=2, iterations=1, ls_kernel=2))
     assert "bytes of shared memory, device allows" in str(e.value)
+
+
+# 4096 < n: the streamed K <= 8 descent, state in shared memory (n * 16 B fits) and in L2 (it does not)
+@pytest.mark.parametrize("n,k,density", [(4500, 2, 0.3), (5000, 8, 0.2), (9000, 3, 0.1), (13000, 6, 0.05),
+                                         (20000, 5, 0.02)])
+def test_streamed_descent_matches_oracle(ccb, oracle, cuda_device, n, k, density):
+    bits, edges = oracle.erdos_renyi(n, density, n + k)
+    p = dict(k=k, population=4, iterations=2, early_stop=10, gww=0.25, seed=5)
+    want = oracle.pbils(bits, edges, make_params(**p))
+    got = ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, **p))
+    _same(got, want, (n, k))
