@@ -5,9 +5,10 @@
 // For each owned vertex u a thread keeps K 32-bit keys
 //     key_c(u) = 16 h_c(u) + c  (+ 2^20 for c = the label of u),   h_c(u) = size_c - 2 G_c(u),
 // so the key of moving u to c orders candidates by h, then by the lower cluster: the reference's rule
-// (MoveDelta, cc_math.hpp:75-77: the gain of a -> c is h_c - h_a + 1).  The 2^20 penalty exceeds the
-// spread 48 n + 15 of unpenalised keys for n <= 21844, so over the K lanes the minimum is the best foreign
-// target and the maximum is the vertex's own cluster: no label, no G, no per-cluster offset is stored.
+// (MoveDelta, cc_math.hpp:75-77: the gain of a -> c is h_c - h_a + 1).  A foreign h_c <= n - size_a and the
+// own h_a >= 2 - size_a, so foreign minus own h is at most n - 2 < 2^15 on the narrow path; the penalty
+// (2^16 in units of h) therefore makes the minimum over the K lanes the best foreign target and the
+// maximum the vertex's own cluster: no label, no G, no per-cluster offset is stored.
 //
 // A move (v: from -> to) shifts, for every vertex u, key_from by +16 if u is a neighbour of v and -16
 // otherwise (size_from - 1, and G_from - 1 for neighbours), and key_to by the opposite amount; with the
@@ -23,7 +24,23 @@
 namespace ccb {
 
 constexpr int kRegPenalty = 1 << 20;
-constexpr int kRegMaxVertices = 21844;  // 48 n + 15 < 2^20
+
+// Minimum and maximum of K lanes with three-input min / max (DPX on sm_90 and later).
+template <int K>
+__device__ __forceinline__ void LanesMinMax(const int* x, int& lo, int& hi) {
+  lo = x[0];
+  hi = x[0];
+  int c = 1;
+#pragma unroll
+  for (; c + 1 < K; c += 2) {
+    lo = __vimin3_s32(lo, x[c], x[c + 1]);
+    hi = __vimax3_s32(hi, x[c], x[c + 1]);
+  }
+  if (c < K) {
+    lo = min(lo, x[c]);
+    hi = max(hi, x[c]);
+  }
+}
 
 template <int K, int T, int V, bool kSmemRows>
 __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t> a) {
@@ -82,7 +99,7 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
         const int gc = ok ? g_src[static_cast<size_t>(c) * ld + u] : 0;
         key[j][c] = s16[c] - 32 * gc + (c == own ? kRegPenalty : 0);
       }
-      ucode[j] = ((1 << bits) << bits) | u;
+      ucode[j] = ok ? (((1 << bits) << bits) | u) : (1 << 30);
     }
   }
   long long objective = a.cur.f[w];
@@ -96,6 +113,7 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
   for (int c = 0; c < K; ++c) coef[c] = 0;
   const uint32_t* prev_row = rows;
   const uint32_t lane_bit = 1u << lane;
+  const uint32_t no_move = (1u << bits) << bits;
 
   while (true) {
     uint32_t rw[V];
@@ -108,22 +126,19 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
       const int d = (rw[j] & lane_bit) ? 16 : -16;
 #pragma unroll
       for (int c = 0; c < K; ++c) key[j][c] += coef[c] * d;
-      int kmin = key[j][0], kmax = key[j][0];
-#pragma unroll
-      for (int c = 1; c < K; ++c) {
-        kmin = min(kmin, key[j][c]);
-        kmax = max(kmax, key[j][c]);
-      }
+      int kmin, kmax;
+      LanesMinMax<K>(key[j], kmin, kmax);
       const int gain = (kmin >> 4) - (kmax >> 4) + (kRegPenalty >> 4) + 1;
-      const uint32_t mk = (gain < 0 && ((valid >> j) & 1)) ? static_cast<uint32_t>(gain * (1 << bits) + ucode[j])
-                                                           : KeyTraits<uint32_t>::kNone;
+      // (gain + 2^B) << B | u for every vertex: improving moves sort below 2^(2B), the rest above it
+      // (gain <= n - 1), and absent vertices carry 2^31 in ucode.
+      const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + static_cast<uint32_t>(ucode[j]);
       if (mk < best) {
         best = mk;
         payload = static_cast<uint32_t>(kmax & 15) | (static_cast<uint32_t>(kmin & 15) << 8);
       }
     }
     const MoveRecord<uint32_t> m = BlockArgMin<uint32_t, kWarps>(best, payload, s_records + parity * kWarps);
-    if (m.key == KeyTraits<uint32_t>::kNone) break;
+    if (m.key >= no_move) break;
     parity ^= 1;
 
     const int v = MoveVertex(m.key, bits);
@@ -155,9 +170,8 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
 #pragma unroll
   for (int j = 0; j < V; ++j) {
     if ((valid >> j) & 1) {
-      int kmax = key[j][0];
-#pragma unroll
-      for (int c = 1; c < K; ++c) kmax = max(kmax, key[j][c]);
+      int kmin, kmax;
+      LanesMinMax<K>(key[j], kmin, kmax);
       dst[tid + j * T] = static_cast<uint8_t>(kmax & 15);
     }
   }

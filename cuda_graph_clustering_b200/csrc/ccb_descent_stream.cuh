@@ -15,6 +15,7 @@
 
 #include <cstdint>
 
+#include "ccb_descent_registers.cuh"
 #include "ccb_descent_small_k.cuh"
 #include "ccb_device.cuh"
 
@@ -31,18 +32,15 @@ __device__ __forceinline__ int SignedLane32(const typename PackedGains<KP>::Vec&
 }
 
 template <int K, int KP, int C>
-struct LaneMinMax {
-  __device__ __forceinline__ static void Run(const typename PackedGains<KP>::Vec& v, const int* off, int& lo,
-                                             int& hi) {
-    const int key = off[C] - SignedLane32<KP, C>(v);
-    lo = min(lo, key);
-    hi = max(hi, key);
-    LaneMinMax<K, KP, C + 1>::Run(v, off, lo, hi);
+struct LaneKeys {
+  __device__ __forceinline__ static void Run(const typename PackedGains<KP>::Vec& v, const int* off, int* keys) {
+    keys[C] = off[C] - SignedLane32<KP, C>(v);
+    LaneKeys<K, KP, C + 1>::Run(v, off, keys);
   }
 };
 template <int K, int KP>
-struct LaneMinMax<K, KP, K> {
-  __device__ __forceinline__ static void Run(const typename PackedGains<KP>::Vec&, const int*, int&, int&) {}
+struct LaneKeys<K, KP, K> {
+  __device__ __forceinline__ static void Run(const typename PackedGains<KP>::Vec&, const int*, int*) {}
 };
 
 template <int KP>
@@ -153,21 +151,22 @@ __global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a)
             P::Add(v[i], delta);
             gv[u] = v[i];
           }
-          int lo = 0x7fffffff, hi = -0x7fffffff;
-          LaneMinMax<K, KP, 0>::Run(v[i], off, lo, hi);
+          int keys[K];
+          LaneKeys<K, KP, 0>::Run(v[i], off, keys);
+          int lo, hi;
+          LanesMinMax<K>(keys, lo, hi);
           const int gain = (lo >> 4) - (hi >> 4) + (kPenalty >> 4) + 1;
-          if (gain < 0) {
-            const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
-            if (mk < best) {
-              best = mk;
-              payload = static_cast<uint32_t>(hi & 15) | (static_cast<uint32_t>(lo & 15) << 8);
-            }
+          // improving moves sort below 2^(2B), the rest above it (gain <= n - 1 keeps it below 2^32)
+          const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
+          if (mk < best) {
+            best = mk;
+            payload = static_cast<uint32_t>(hi & 15) | (static_cast<uint32_t>(lo & 15) << 8);
           }
         }
       }
     }
     const MoveRecord<uint32_t> m = BlockArgMin<uint32_t, kWarps>(best, payload, s_records + parity * kWarps);
-    if (m.key == KeyTraits<uint32_t>::kNone) break;
+    if (m.key >= key_base) break;
     parity ^= 1;
 
     const int v = MoveVertex(m.key, bits);
