@@ -2,6 +2,7 @@
 // so that the many template instances compile in parallel with the rest of the library.
 #include <cuda_runtime.h>
 
+#include "ccb_descent_incremental.cuh"
 #include "ccb_descent_registers.cuh"
 #include "ccb_descent_stream.cuh"
 #include "ccb_plans.h"
@@ -57,7 +58,32 @@ cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int 
                       : GoStream<K, 1024, false>(a, grid, p.smem_bytes, st, cfg);
 }
 
+template <int T, bool S>
+cudaError_t GoIncremental(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_incremental<T, S>;
+  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel<<<grid, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+size_t IncrementalBytes(int k, int ld) { return IncState::Bytes(k, ld); }
+
+cudaError_t LaunchDescentIncremental(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st,
+                                     bool configure) {
+  switch (p.threads) {
+    case 256:
+      return p.smem_state ? GoIncremental<256, true>(a, grid, p.smem_bytes, st, configure)
+                          : GoIncremental<256, false>(a, grid, p.smem_bytes, st, configure);
+    case 512:
+      return p.smem_state ? GoIncremental<512, true>(a, grid, p.smem_bytes, st, configure)
+                          : GoIncremental<512, false>(a, grid, p.smem_bytes, st, configure);
+    default:
+      return p.smem_state ? GoIncremental<1024, true>(a, grid, p.smem_bytes, st, configure)
+                          : GoIncremental<1024, false>(a, grid, p.smem_bytes, st, configure);
+  }
+}
 
 size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows) {
   (void)pitch;

@@ -24,6 +24,11 @@ size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state,
 int SmallKLanes(int k);
 size_t RegistersSmem(int n, int pitch, bool smem_rows);
 bool RegistersShapeBuilt(int threads, int vpt);
+// Incremental descent for 9 <= k <= 64 (ccb_descent_incremental.cuh): SmallKPlan fields threads,
+// smem_state and smem_bytes apply; k is the runtime cluster count.
+size_t IncrementalBytes(int k, int ld);
+cudaError_t LaunchDescentIncremental(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
+                                     cudaStream_t stream, bool configure);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);
 

@@ -214,7 +214,8 @@ struct Plan {
   int threads = 512;
   size_t smem_bytes = 0;
   int key_bits = 0;
-  bool small_k = false;     // the packed K <= 8 descent (ccb_descent_small_k.cuh)
+  bool small_k = false;     // the packed K <= 8 descents (registers / streamed)
+  bool incremental = false; // the incremental 9 <= k <= 64 descent
   SmallKPlan sk;
 };
 
@@ -296,6 +297,18 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
     p.threads = sk.threads;
     p.smem_bytes = sk.smem_bytes;
   }
+  if (!p.wide && k > 8 && ls_kernel == CCB_LS_AUTO) {
+    SmallKPlan& sk = p.sk;
+    sk.k = k;
+    sk.threads = n <= 2048 ? 256 : (n <= 8192 ? 512 : 1024);
+    sk.smem_state = IncrementalBytes(k, ld) + 10 * 1024 <= limit;  // the kernel's static shared memory
+    sk.smem_bytes = sk.smem_state ? IncrementalBytes(k, ld) : 0;
+    p.incremental = true;
+    p.smem_state = sk.smem_state;
+    p.smem_rows = false;
+    p.threads = sk.threads;
+    p.smem_bytes = sk.smem_bytes;
+  }
   return p;
 }
 
@@ -338,6 +351,7 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 }
 
 const char* KernelName(const Plan& p) {
+  if (p.incremental) return p.smem_state ? "incremental 9 <= k <= 64, shared memory" : "incremental 9 <= k <= 64, L2";
   if (p.small_k) {
     if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
                                            : "packed k <= 8, registers";
@@ -484,8 +498,11 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   const size_t labels = (size_t)pop * s->ld;
   const size_t gains = labels * k;
   const size_t gb = s->GainBytes();
-  const size_t next_lanes = s->plan.smem_state ? 0 : (s->plan.small_k ? std::max(k, SmallKLanes(k)) : k);
-  size_t bytes = 2 * labels + gains * gb + labels * next_lanes * gb + (size_t)pop * s->kpad * 4 + 2 * pop * 8 +
+  const size_t next_bytes =
+      s->plan.smem_state ? 0
+                         : (s->plan.incremental ? (size_t)pop * IncrementalBytes(k, s->ld)
+                                                : labels * (s->plan.small_k ? std::max(k, SmallKLanes(k)) : k) * gb);
+  size_t bytes = 2 * labels + gains * gb + next_bytes + (size_t)pop * s->kpad * 4 + 2 * pop * 8 +
                  (size_t)pop * k * g->pitch * 4 + 2 * (size_t)pop * 4 + s->ld + sizeof(Control);
   size_t free_b = 0, total_b = 0;
   CCB_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -500,9 +517,10 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->cur_g = cg;
   if (!s->plan.smem_state) {
     // the global-state descents work in the slot's rows of next: cluster-major G, or packed vectors
-    const size_t lanes = s->plan.small_k ? std::max(k, SmallKLanes(k)) : k;
+    const size_t bytes_next = s->plan.incremental ? (size_t)pop * IncrementalBytes(k, s->ld)
+                                                  : labels * (s->plan.small_k ? std::max(k, SmallKLanes(k)) : k) * gb;
     uint8_t* ng = nullptr;
-    s->Alloc(ng, labels * lanes * gb);
+    s->Alloc(ng, bytes_next);
     s->next_g = ng;
   }
   s->Alloc(s->cur_sizes, (size_t)pop * s->kpad);
@@ -521,7 +539,9 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   CCB_CUDA(cudaEventCreateWithFlags(&s->poll_event[1], cudaEventDisableTiming));
 
   // Shared-memory opt-in for the descent instance of this plan.
-  if (s->plan.small_k) {
+  if (s->plan.incremental) {
+    CCB_CUDA(LaunchDescentIncremental(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
+  } else if (s->plan.small_k) {
     CCB_CUDA(LaunchDescentSmallK(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
   } else if (s->plan.wide) {
     LaunchDescent<int32_t>(s->plan, DescentArgs<int32_t>{}, 0, nullptr, true);
@@ -575,9 +595,12 @@ void LaunchDescentStep(ccb_solver& s, int grid, int population, int tournament, 
   a.iteration = iteration;
   a.select_stream = stream;
   if constexpr (std::is_same_v<GainT, int16_t>) {
-    if (s.plan.small_k) {
+    if (s.plan.small_k || s.plan.incremental) {
       cudaError_t e = cudaSuccess;
-      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentSmallK(s.plan.sk, a, grid, st, false); });
+      s.timer.Time(kCatDescent, st, [&] {
+        e = s.plan.incremental ? LaunchDescentIncremental(s.plan.sk, a, grid, st, false)
+                               : LaunchDescentSmallK(s.plan.sk, a, grid, st, false);
+      });
       CCB_CUDA(e);
       return;
     }

@@ -218,9 +218,11 @@ def test_shared_kernel_rejects_oversized_state(ccb, oracle, cuda_device):
     assert "bytes of shared memory, device allows" in str(e.value)
 
 
-# 4096 < n: the streamed K <= 8 descent, state in shared memory (n * 16 B fits) and in L2 (it does not)
+# 4096 < n: the streamed K <= 8 descent, state in shared memory (n * 16 B fits) and in L2 (it does not);
+# k > 8: the incremental descent, state in shared memory (n <= ~1500 at k = 12) and in L2
 @pytest.mark.parametrize("n,k,density", [(4500, 2, 0.3), (5000, 8, 0.2), (9000, 3, 0.1), (13000, 6, 0.05),
-                                         (20000, 5, 0.02)])
+                                         (20000, 5, 0.02), (1500, 12, 0.3), (3000, 40, 0.1), (6000, 20, 0.05),
+                                         (2500, 64, 0.5)])
 def test_streamed_descent_matches_oracle(ccb, oracle, cuda_device, n, k, density):
     bits, edges = oracle.erdos_renyi(n, density, n + k)
     p = dict(k=k, population=4, iterations=2, early_stop=10, gww=0.25, seed=5)
