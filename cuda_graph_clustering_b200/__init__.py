@@ -19,7 +19,7 @@ from ._native import (CcbError, CcbParams, CcbResult, CcbKernelStats, LS_AUTO, L
                       MAX_CLUSTERS, MAX_VERTICES_NARROW, MAX_VERTICES_WIDE, check, lib)
 
 __all__ = ["Graph", "PbilsParams", "PbilsResult", "SolveGpu", "SolveNeighborhoodGpu",
-           "SolveNeighborhoodWithManyLocalSearchesGpu", "DeviceGraph", "Solver", "CcbError", "LS_AUTO", "LS_GLOBAL",
+           "SolveNeighborhoodWithManyLocalSearchesGpu", "DeviceGraph", "Solver", "Batch", "CcbError", "LS_AUTO", "LS_GLOBAL",
            "LS_SHARED", "LS_WIDE", "MAX_CLUSTERS", "kMaxClusters"]
 
 kMaxClusters = MAX_CLUSTERS  # include/cc_gpu.hpp:10
@@ -167,6 +167,39 @@ class DeviceGraph:
             self.n, self.edges = n, edges
         self.handle = h
 
+    @classmethod
+    def _wrap(cls, handle: C.c_void_p) -> "DeviceGraph":
+        g = cls.__new__(cls)
+        g.handle = handle
+        n = C.c_uint32()
+        e = C.c_uint64()
+        check(lib().ccb_graph_size(handle, C.byref(n), C.byref(e)))
+        g.n, g.edges = int(n.value), int(e.value)
+        return g
+
+    @classmethod
+    def erdos_renyi(cls, n: int, density: float, seed: int, stream: int = 0) -> "DeviceGraph":
+        """Graph::ErdosRenyi generated on the device (same bits as the host generator)."""
+        h = C.c_void_p()
+        check(lib().ccb_graph_generate_erdos_renyi(n, density, seed, stream or None, C.byref(h)))
+        return cls._wrap(h)
+
+    @classmethod
+    def planted(cls, n: int, parts: int, p_in: float, p_out: float, flip: float, seed: int,
+                shuffle_split: bool = False, stream: int = 0) -> tuple["DeviceGraph", np.ndarray]:
+        """The planted partition generated on the device (same bits as Graph.Planted)."""
+        h = C.c_void_p()
+        comm = np.zeros(max(n, 1), np.int32)
+        check(lib().ccb_graph_generate_planted(n, parts, int(shuffle_split), p_in, p_out, flip, seed, stream or None,
+                                               C.byref(h), comm.ctypes.data))
+        return cls._wrap(h), comm[:n]
+
+    def download(self) -> Graph:
+        w = words_per_row(self.n)
+        bits = np.zeros((max(self.n, 1), w), np.uint32)
+        check(lib().ccb_graph_download(self.handle, bits.ctypes.data, w))
+        return Graph(self.n, bits[: self.n], self.edges)
+
     def close(self) -> None:
         if self.handle:
             lib().ccb_graph_destroy(self.handle)
@@ -243,3 +276,48 @@ def evaluate_labelings_noalloc(bits_ptr: int, n: int, words_per_row: int, edges:
     its scratch is a fixed 4 MiB device array (count * k * ceil(n / 32) <= 1048576 mask words)."""
     check(lib().ccb_evaluate_labelings_noalloc(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr,
                                                sizes_ptr, g_ptr, stream or None))
+
+
+class Batch:
+    """Many independent PBILS instances solved together (ccb_batch_*): one CUDA graph per iteration of all
+    instances, persistent per-bucket descent kernels fed by a device work queue.  Each result equals the
+    instance's plain solve bit for bit."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib().ccb_batch_create(C.byref(h)))
+        self.handle = h
+        self.graphs = []
+        self.sizes = []
+
+    def add(self, graph: DeviceGraph, params: PbilsParams) -> int:
+        p = params.to_c()
+        i = C.c_int32()
+        check(lib().ccb_batch_add(self.handle, graph.handle, C.byref(p), C.byref(i)))
+        self.graphs.append(graph)
+        self.sizes.append(graph.n)
+        return int(i.value)
+
+    def run(self) -> None:
+        check(lib().ccb_batch_run(self.handle))
+
+    def result(self, i: int) -> PbilsResult:
+        n = self.sizes[i]
+        labels = np.zeros(max(n, 1), np.int32)
+        res = CcbResult()
+        check(lib().ccb_batch_result(self.handle, i, labels.ctypes.data, C.byref(res)))
+        return PbilsResult.from_c(res, labels[:n])
+
+    def describe(self) -> str:
+        return lib().ccb_batch_describe(self.handle).decode()
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ccb_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -65,6 +65,16 @@ SIGNATURES = {
     "ccb_solver_destroy": (None, [_vp]),
     "ccb_solver_set_profiling": (C.c_int, [_vp, C.c_int32]),
     "ccb_solver_stats": (C.c_int, [_vp, C.POINTER(CcbKernelStats)]),
+    "ccb_graph_generate_erdos_renyi": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _vp, C.POINTER(_vp)]),
+    "ccb_graph_generate_planted": (C.c_int, [C.c_uint32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                             C.c_uint64, _vp, C.POINTER(_vp), _vp]),
+    "ccb_graph_download": (C.c_int, [_vp, _vp, C.c_uint32]),
+    "ccb_batch_create": (C.c_int, [C.POINTER(_vp)]),
+    "ccb_batch_add": (C.c_int, [_vp, _vp, C.POINTER(CcbParams), C.POINTER(C.c_int32)]),
+    "ccb_batch_run": (C.c_int, [_vp]),
+    "ccb_batch_result": (C.c_int, [_vp, C.c_int32, _vp, C.POINTER(CcbResult)]),
+    "ccb_batch_describe": (C.c_char_p, [_vp]),
+    "ccb_batch_destroy": (None, [_vp]),
     "ccb_evaluate_labelings": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, _vp, _vp,
                                          _vp, _vp, _vp]),
     "ccb_evaluate_labelings_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32,

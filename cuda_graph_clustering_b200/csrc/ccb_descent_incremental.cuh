@@ -49,7 +49,7 @@ struct IncState {
 };
 
 template <int T, bool kSmemState>
-__global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_t> a) {
+__device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a, int slot) {
   constexpr int kWarps = T / kWarp;
   constexpr int U = 4;
   constexpr int KP = kMaxK;
@@ -59,7 +59,6 @@ __global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_
   __shared__ MoveRecord<uint32_t> s_records[2 * kWarps];
   __shared__ int s_off[kWarps][KP];
 
-  const int slot = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid % kWarp;
   const int warp = tid / kWarp;
@@ -204,6 +203,12 @@ __global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_
     a.next.f[slot] = objective;
     if (applied) atomicAdd(&a.ctl->moves, applied);
   }
+}
+
+// One slot per block (plain path).
+template <int T, bool kSmemState>
+__global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_t> a) {
+  DescentIncremental<T, kSmemState>(a, blockIdx.x);
 }
 
 }  // namespace ccb

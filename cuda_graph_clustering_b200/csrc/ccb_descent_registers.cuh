@@ -43,14 +43,13 @@ __device__ __forceinline__ void LanesMinMax(const int* x, int& lo, int& hi) {
 }
 
 template <int K, int T, int V, bool kSmemRows>
-__global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t> a) {
+__device__ __forceinline__ void DescentRegisters(const DescentArgs<int16_t>& a, int slot) {
   constexpr int kWarps = T / kWarp;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
   __shared__ int s_stop;
   __shared__ MoveRecord<uint32_t> s_records[2 * kWarps];
 
-  const int slot = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid % kWarp;
   const int n = a.gr.n;
@@ -179,6 +178,12 @@ __global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t>
     a.next.f[slot] = objective;
     if (applied) atomicAdd(&a.ctl->moves, applied);
   }
+}
+
+// One slot per block (plain path).
+template <int K, int T, int V, bool kSmemRows>
+__global__ void __launch_bounds__(T, 1) k_descent_registers(DescentArgs<int16_t> a) {
+  DescentRegisters<K, T, V, kSmemRows>(a, blockIdx.x);
 }
 
 }  // namespace ccb

@@ -52,7 +52,7 @@ __device__ __forceinline__ void ShiftLane(typename PackedGains<KP>::Vec& v, int 
 }
 
 template <int K, int T, bool kSmemState>
-__global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a) {
+__device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int slot) {
   constexpr int KP = PackedLanes(K);
   constexpr int U = 4;  // vertices in flight per thread
   using P = PackedGains<KP>;
@@ -64,7 +64,6 @@ __global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a)
   __shared__ int s_stop;
   __shared__ MoveRecord<uint32_t> s_records[2 * kWarps];
 
-  const int slot = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid % kWarp;
   const int n = a.gr.n;
@@ -208,6 +207,12 @@ __global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a)
     a.next.f[slot] = objective;
     if (applied) atomicAdd(&a.ctl->moves, applied);
   }
+}
+
+// One slot per block (plain path).
+template <int K, int T, bool kSmemState>
+__global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a) {
+  DescentStream<K, T, kSmemState>(a, blockIdx.x);
 }
 
 }  // namespace ccb

@@ -23,6 +23,8 @@ struct Control {
   unsigned long long t0_ns; // %globaltimer at solve start, for the device-side time limit
   int32_t record_slot;      // slot the record last came from
   int32_t error;            // nonzero when a bounded device-side wait gave up
+  int32_t iter;             // current iteration of a batched instance (the plain path passes it as argument)
+  int32_t pad;
 };
 
 // One line of the --verbose progress log, written by the record kernel.

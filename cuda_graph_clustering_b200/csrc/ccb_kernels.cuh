@@ -29,11 +29,11 @@ enum RebuildMode : int {
   kRebuildNeighborhood = 3 // cur[s] = {v, N(v)} vs rest with v = first + s
 };
 
-__global__ void k_mark_start(Control* ctl) {
+static __global__ void k_mark_start(Control* ctl) {
   ctl->t0_ns = GlobalTimerNs();
 }
 
-__global__ void k_degrees(const uint32_t* __restrict__ bits, int n, int words, int pitch, int32_t* degrees) {
+static __global__ void k_degrees(const uint32_t* __restrict__ bits, int n, int words, int pitch, int32_t* degrees) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   const uint32_t* row = bits + static_cast<size_t>(v) * pitch;
@@ -43,7 +43,7 @@ __global__ void k_degrees(const uint32_t* __restrict__ bits, int n, int words, i
 }
 
 // labels[slot][v] = InitialLabel(stream, slot * n + v, k) over a grid-stride loop.
-__global__ void k_init_labels(uint8_t* labels, int pop, int n, int ld, int k, uint64_t stream) {
+static __global__ void k_init_labels(uint8_t* labels, int pop, int n, int ld, int k, uint64_t stream) {
   const long long total = static_cast<long long>(pop) * n;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -58,19 +58,43 @@ __global__ void k_init_labels(uint8_t* labels, int pop, int n, int ld, int k, ui
 // through L1), phase 3 gives each warp whole rows: lanes stride over the row's words, AND it with the
 // masks of a chunk of clusters, count bits, and reduce across the warp in hardware.  The last
 // cluster's row of G is the degree minus the others, so only k - 1 masks are intersected.
+template <typename GainT>
+struct RebuildArgs {
+  GraphView gr;
+  PopView<GainT> cur;
+  const uint8_t* next_labels;
+  const int32_t* src_map;
+  uint32_t* masks;
+  int k;
+  int kpad;
+  int ld;
+  int mode;
+  uint64_t stream;
+  int iteration;
+  float probability;
+  int first;
+  const Control* ctl;  // checked for the stop flag in the perturb / copy modes (may be null)
+};
+
 template <typename GainT, int kThreads>
-__global__ void __launch_bounds__(kThreads) k_rebuild(GraphView gr, PopView<GainT> cur, const uint8_t* __restrict__ next_labels,
-                                                      const int32_t* __restrict__ src_map, uint32_t* __restrict__ masks,
-                                                      int k, int kpad, int ld, int mode, uint64_t stream,
-                                                      int iteration, float probability, int first,
-                                                      const Control* __restrict__ ctl) {
+__device__ __forceinline__ void RebuildBody(const RebuildArgs<GainT>& a, int slot) {
+  const GraphView& gr = a.gr;
+  const PopView<GainT>& cur = a.cur;
+  const uint8_t* __restrict__ next_labels = a.next_labels;
+  const int32_t* __restrict__ src_map = a.src_map;
+  uint32_t* __restrict__ masks = a.masks;
+  const int k = a.k, kpad = a.kpad, ld = a.ld, mode = a.mode;
+  const uint64_t stream = a.stream;
+  const int iteration = a.iteration;
+  const float probability = a.probability;
+  const int first = a.first;
+  const Control* ctl = a.ctl;
   constexpr int kWarps = kThreads / kWarp;
   constexpr int kChunk = 8;
   __shared__ int s_sizes[kMaxK];
   __shared__ long long s_sum[kWarps];
   if (ctl != nullptr && (mode == kRebuildPerturb || mode == kRebuildCopy) && ctl->stop) return;
 
-  const int slot = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid % kWarp;
   const int warp = tid / kWarp;
@@ -157,6 +181,11 @@ __global__ void __launch_bounds__(kThreads) k_rebuild(GraphView gr, PopView<Gain
     cur.f[slot] = gr.edges + pairs - sum;
   }
   for (int c = tid; c < k; c += kThreads) cur.sizes[static_cast<size_t>(slot) * kpad + c] = s_sizes[c];
+}
+
+template <typename GainT, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_rebuild(RebuildArgs<GainT> a) {
+  RebuildBody<GainT, kThreads>(a, blockIdx.x);
 }
 
 // Steepest descent of one slot per block until no strictly improving single-vertex move remains.
@@ -345,7 +374,7 @@ struct RecordArgs {
 // (cc_pbils.hpp:69-78); the GWW map ranks slots by (f, slot) as RankSlots does
 // (cc_pbils_cpu.cpp:170-175) and sends the i-th best to the i-th worst for i < copies.
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads) k_record(RecordArgs a) {
+__device__ __forceinline__ void RecordBody(const RecordArgs& a) {
   constexpr int kWarps = kThreads / kWarp;
   __shared__ long long s_f[kWarps];
   __shared__ int s_slot[kWarps];
@@ -425,6 +454,11 @@ __global__ void __launch_bounds__(kThreads) k_record(RecordArgs a) {
   }
   __syncthreads();
   for (int i = tid; i < a.copies; i += kThreads) a.src_map[a.order[a.count - 1 - i]] = a.order[i];
+}
+
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) k_record(RecordArgs a) {
+  RecordBody<kThreads>(a);
 }
 
 }  // namespace ccb

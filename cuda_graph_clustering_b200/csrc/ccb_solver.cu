@@ -12,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <tuple>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -20,7 +22,9 @@
 #include <vector>
 
 #include "ccb.h"
+#include "ccb_batch.h"
 #include "ccb_error.h"
+#include "ccb_util.h"
 #include "ccb_kernels.cuh"
 #include "ccb_plans.h"
 
@@ -38,40 +42,6 @@ void SetLastError(const char* message) {
 const char* LastError() { return g_last_error; }
 
 namespace {
-
-struct Failure {
-  int status;
-  std::string message;
-};
-
-#define CCB_CUDA(call)                                                                                     \
-  do {                                                                                                     \
-    const cudaError_t e_ = (call);                                                                         \
-    if (e_ != cudaSuccess) {                                                                               \
-      throw ::ccb::Failure{CCB_ERR_CUDA, std::string("cuda error at ") + __FILE__ + ":" +                  \
-                                             std::to_string(__LINE__) + ": " + cudaGetErrorString(e_)};    \
-    }                                                                                                      \
-  } while (0)
-
-[[noreturn]] void Fail(int status, const std::string& message) { throw Failure{status, message}; }
-
-template <typename F>
-int Guard(F&& body) {
-  try {
-    body();
-    g_last_error[0] = '\0';
-    return CCB_OK;
-  } catch (const Failure& e) {
-    SetLastError(e.message);
-    return e.status;
-  } catch (const std::bad_alloc&) {
-    SetLastError("host memory exhausted");
-    return CCB_ERR_DEVICE_MEMORY;
-  } catch (const std::exception& e) {
-    SetLastError(e.what());
-    return CCB_ERR_INVALID;
-  }
-}
 
 constexpr int kAuxThreads = 256;
 constexpr int kRebuildThreads = 512;
@@ -146,61 +116,23 @@ int CountClustersUsed(const int32_t* labels, uint32_t n, int k) {
 
 using namespace ccb;
 
-// ------------------------------------------------------------------------------------------------
-// Device graph
-// ------------------------------------------------------------------------------------------------
-struct ccb_graph {
-  int device = 0;
-  int n = 0;
-  int words = 0;  // ceil(n / 32)
-  int pitch = 0;  // words per row in memory (multiple of 4)
-  int64_t edges = 0;
-  uint32_t* bits = nullptr;
-  int32_t* degrees = nullptr;
-
-  GraphView View() const { return GraphView{bits, degrees, n, words, pitch, edges}; }
-  ~ccb_graph() {
-    if (bits) cudaFree(bits);
-    if (degrees) cudaFree(degrees);
-  }
-};
+#include "ccb_graph.h"
 
 namespace {
 
 ccb_graph* MakeGraph(const uint32_t* src, bool src_on_device, uint32_t n, uint32_t words_per_row, uint64_t edges,
                      cudaStream_t stream) {
-  if (n > (uint32_t)CCB_MAX_VERTICES_WIDE) {
-    Fail(CCB_ERR_INVALID, "n exceeds " + std::to_string(CCB_MAX_VERTICES_WIDE) + ", the range of the packed move");
-  }
   const int words = (int)((n + 31) / 32);
   if (n > 0 && words_per_row < (uint32_t)words) Fail(CCB_ERR_INVALID, "words_per_row < ceil(n / 32)");
   if (n > 0 && src == nullptr) Fail(CCB_ERR_INVALID, "null bitset");
-  std::unique_ptr<ccb_graph> g(new ccb_graph());
-  CCB_CUDA(cudaGetDevice(&g->device));
-  g->n = (int)n;
-  g->words = words;
-  g->pitch = std::max(4, (words + 3) / 4 * 4);
+  std::unique_ptr<ccb_graph> g(AllocateGraph(n, stream));
   g->edges = (int64_t)edges;
-  const size_t rows = std::max<uint32_t>(n, 1);
-  const size_t bytes = rows * g->pitch * sizeof(uint32_t);
-  size_t free_b = 0, total_b = 0;
-  CCB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if (bytes + rows * 4 > free_b) {
-    Fail(CCB_ERR_DEVICE_MEMORY, "graph needs " + Mebibytes(bytes) + " of device memory, " + Mebibytes(free_b) + " free");
-  }
-  CCB_CUDA(cudaMalloc(&g->bits, bytes));
-  CCB_CUDA(cudaMalloc(&g->degrees, rows * sizeof(int32_t)));
-  CCB_CUDA(cudaMemsetAsync(g->bits, 0, bytes, stream));
-  CCB_CUDA(cudaMemsetAsync(g->degrees, 0, rows * sizeof(int32_t), stream));
   if (n > 0) {
     CCB_CUDA(cudaMemcpy2DAsync(g->bits, g->pitch * sizeof(uint32_t), src, words_per_row * sizeof(uint32_t),
                                words * sizeof(uint32_t), n,
                                src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
-    k_degrees<<<(int)CeilDiv(n, kAuxThreads), kAuxThreads, 0, stream>>>(g->bits, (int)n, words, g->pitch,
-                                                                         g->degrees);
-    CCB_CUDA(cudaGetLastError());
   }
-  CCB_CUDA(cudaStreamSynchronize(stream));
+  FinishGraph(*g, stream);
   return g.release();
 }
 
@@ -570,11 +502,9 @@ template <typename GainT>
 void LaunchRebuild(ccb_solver& s, int grid, int mode, const int32_t* src_map, uint64_t stream, int iteration,
                    float prob, int first, bool check_stop, cudaStream_t st) {
   if (grid <= 0) return;
-  s.timer.Time(kCatRebuild, st, [&] {
-    k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(
-        s.graph->View(), s.Cur<GainT>(), s.next_lab, src_map, s.masks, s.k, s.kpad, s.ld, mode, stream, iteration,
-        prob, first, check_stop ? s.ctl : nullptr);
-  });
+  const RebuildArgs<GainT> a{s.graph->View(), s.Cur<GainT>(), s.next_lab, src_map, s.masks, s.k, s.kpad, s.ld,
+                             mode, stream, iteration, prob, first, check_stop ? s.ctl : nullptr};
+  s.timer.Time(kCatRebuild, st, [&] { k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(a); });
   CCB_CUDA(cudaGetLastError());
 }
 
@@ -788,6 +718,351 @@ void CheckSolverMatches(const ccb_solver* s, const ccb_params& p) {
 }  // namespace
 
 // ------------------------------------------------------------------------------------------------
+// Batched engine: many instances, one CUDA graph per PBILS iteration, persistent bucket kernels
+// ------------------------------------------------------------------------------------------------
+struct ccb_batch {
+  struct Instance {
+    const ccb_graph* graph = nullptr;
+    ccb_params params{};
+    std::unique_ptr<ccb_solver> solver;
+    bool batched = false;  // false: solved on the plain path (k = 1, n = 0)
+    ccb_result result{};
+    std::vector<int32_t> labels;
+  };
+  struct Bucket {
+    BatchShape shape;
+    std::vector<int> members;  // entry indices, heaviest first
+    int total = 0;
+    size_t offset = 0;         // of the member list in the device list buffer (int32 units)
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+  };
+  Device device;
+  std::vector<Instance> inst;
+  std::vector<Bucket> buckets;
+  std::vector<int> entry_of;   // instance -> entry (-1 if not batched)
+  std::vector<int> batched;    // entry -> instance
+  BatchEntry* d_entries = nullptr;
+  int32_t* d_lists = nullptr;  // member lists and prefix sums of all queues
+  int32_t* d_heads = nullptr;  // one queue head per bucket + one for the rebuild queue
+  int32_t* d_active = nullptr;
+  int32_t* h_active = nullptr;  // pinned, two slots
+  BatchQueue rebuild_queue{};
+  int rebuild_grid = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t poll[2] = {nullptr, nullptr};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool prepared = false;
+  int max_iterations = 0;
+  long long replays = 0;
+  std::string description;
+
+  ~ccb_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (Bucket& b : buckets) {
+      if (b.stream) cudaStreamDestroy(b.stream);
+      if (b.done) cudaEventDestroy(b.done);
+    }
+    for (cudaEvent_t e : poll)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+    if (d_entries) cudaFree(d_entries);
+    if (d_lists) cudaFree(d_lists);
+    if (d_heads) cudaFree(d_heads);
+    if (d_active) cudaFree(d_active);
+    if (h_active) cudaFreeHost(h_active);
+  }
+};
+
+namespace {
+
+// Work estimate of one slot's descent, for ordering a queue heaviest first.
+double SlotWork(const ccb_solver& s) { return (double)s.n * s.n * std::max(2, std::min(s.k, 8)); }
+
+BatchEntry MakeEntry(const ccb_solver& s, const ccb_params& p) {
+  BatchEntry e{};
+  DescentArgs<int16_t>& d = e.descent;
+  d.gr = s.graph->View();
+  d.cur = s.Cur<int16_t>();
+  d.next = s.Next<int16_t>();
+  d.ctl = s.ctl;
+  d.k = s.k;
+  d.kpad = s.kpad;
+  d.ld = s.ld;
+  d.key_bits = s.plan.key_bits;
+  d.population = s.pop;
+  d.tournament = p.tournament;
+  d.iteration = 0;
+  d.select_stream = StreamSeed(p.seed, kSelectTag, 0);
+  const int copies = (int)(p.gww * s.pop);
+  const bool perturb = s.k >= 2 && p.perturbation > 0.0;
+  e.rebuild = RebuildArgs<int16_t>{s.graph->View(), s.Cur<int16_t>(), s.next_lab, copies > 0 ? s.src_map : nullptr,
+                                   s.masks, s.k, s.kpad, s.ld, perturb ? kRebuildPerturb : kRebuildCopy,
+                                   StreamSeed(p.seed, kPerturbTag, 0), 0, (float)p.perturbation, 0, s.ctl};
+  RecordArgs& r = e.record;
+  r.f = s.next_f;
+  r.labels = s.next_lab;
+  r.ld = s.ld;
+  r.n = s.n;
+  r.count = s.pop;
+  r.ctl = s.ctl;
+  r.record_labels = s.record_lab;
+  r.mode = kRecordIteration;
+  r.early_stop = p.early_stop;
+  r.copies = copies;
+  r.src_map = s.src_map;
+  r.order = s.order;
+  r.trace = nullptr;
+  r.time_limit_ns = p.time_limit_sec > 0 ? (unsigned long long)(p.time_limit_sec * 1e9) : 0ull;
+  e.iterations = p.iterations;
+  return e;
+}
+
+BatchShape ShapeOf(const ccb_solver& s) {
+  BatchShape sh;
+  const SmallKPlan& sk = s.plan.sk;
+  sh.k = s.k;
+  sh.threads = sk.threads;
+  sh.vpt = sk.vpt;
+  if (s.plan.incremental) {
+    sh.kind = kBatchIncremental;
+    sh.k = 0;
+    sh.smem = sk.smem_state;
+  } else if (sk.registers) {
+    sh.kind = kBatchRegisters;
+    sh.smem = sk.smem_rows;
+  } else {
+    sh.kind = kBatchStream;
+    sh.smem = sk.smem_state;
+  }
+  sh.smem_bytes = sk.smem_bytes;
+  return sh;
+}
+
+// Global-memory state bytes per running slot of an L2-streamed bucket (0 when the state is in shared memory).
+size_t L2StateBytes(const ccb_solver& s) {
+  if (s.plan.incremental) return s.plan.smem_state ? 0 : IncrementalBytes(s.k, s.ld);
+  if (!s.plan.sk.registers && !s.plan.smem_state) return (size_t)s.ld * SmallKLanes(s.k) * 2;
+  return 0;
+}
+
+void PrepareBatch(ccb_batch& b) {
+  if (b.prepared) return;
+  if (b.stream == nullptr) CCB_CUDA(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+  b.entry_of.assign(b.inst.size(), -1);
+  b.batched.clear();
+  std::vector<BatchEntry> entries;
+  for (size_t i = 0; i < b.inst.size(); ++i) {
+    ccb_batch::Instance& in = b.inst[i];
+    if (in.graph->n == 0) continue;
+    in.solver.reset(MakeSolver(in.graph, in.params.k, in.params.population, CCB_LS_AUTO));
+    const Plan& pl = in.solver->plan;
+    in.batched = !pl.wide && (pl.small_k || pl.incremental);
+    if (!in.batched) continue;
+    b.entry_of[i] = (int)entries.size();
+    b.batched.push_back((int)i);
+    entries.push_back(MakeEntry(*in.solver, in.params));
+    b.max_iterations = std::max(b.max_iterations, in.params.iterations);
+  }
+  const int count = (int)entries.size();
+  // Buckets: one persistent kernel instance each.
+  std::map<std::tuple<int, int, int, int, int>, int> index;
+  for (int e = 0; e < count; ++e) {
+    const ccb_solver& s = *b.inst[b.batched[e]].solver;
+    const BatchShape sh = ShapeOf(s);
+    const auto key = std::make_tuple(sh.kind, sh.k, sh.threads, sh.vpt, (int)sh.smem);
+    auto it = index.find(key);
+    if (it == index.end()) {
+      it = index.emplace(key, (int)b.buckets.size()).first;
+      b.buckets.emplace_back();
+      b.buckets.back().shape = sh;
+    }
+    ccb_batch::Bucket& bk = b.buckets[it->second];
+    bk.shape.smem_bytes = std::max(bk.shape.smem_bytes, sh.smem_bytes);
+    bk.members.push_back(e);
+  }
+  // Queue layout in one device buffer: per bucket members then prefix, then the rebuild queue.
+  std::vector<int32_t> lists;
+  std::vector<BatchQueue> queues;
+  auto add_queue = [&](std::vector<int>& members) {
+    std::sort(members.begin(), members.end(), [&](int x, int y) {
+      return SlotWork(*b.inst[b.batched[x]].solver) > SlotWork(*b.inst[b.batched[y]].solver);
+    });
+    BatchQueue q{};
+    const size_t at = lists.size();
+    for (int m : members) lists.push_back(m);
+    int total = 0;
+    for (int m : members) {
+      lists.push_back(total);
+      total += b.inst[b.batched[m]].solver->pop;
+    }
+    lists.push_back(total);
+    q.count = (int)members.size();
+    q.total = total;
+    queues.push_back(q);
+    return at;
+  };
+  for (ccb_batch::Bucket& bk : b.buckets) {
+    bk.offset = add_queue(bk.members);
+    bk.total = queues.back().total;
+  }
+  std::vector<int> all(count);
+  for (int e = 0; e < count; ++e) all[e] = e;
+  const size_t rebuild_at = add_queue(all);
+
+  CCB_CUDA(cudaMalloc(&b.d_entries, std::max<size_t>(1, entries.size()) * sizeof(BatchEntry)));
+  CCB_CUDA(cudaMalloc(&b.d_lists, std::max<size_t>(1, lists.size()) * sizeof(int32_t)));
+  CCB_CUDA(cudaMalloc(&b.d_heads, (b.buckets.size() + 1) * sizeof(int32_t)));
+  CCB_CUDA(cudaMalloc(&b.d_active, sizeof(int32_t)));
+  CCB_CUDA(cudaMallocHost(&b.h_active, 2 * sizeof(int32_t)));
+  if (!entries.empty()) {
+    CCB_CUDA(cudaMemcpy(b.d_entries, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice));
+  }
+  if (!lists.empty()) {
+    CCB_CUDA(cudaMemcpy(b.d_lists, lists.data(), lists.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  auto view = [&](size_t at, const BatchQueue& q, int head) {
+    BatchQueue v = q;
+    v.instances = b.d_lists + at;
+    v.prefix = b.d_lists + at + q.count;
+    v.head = b.d_heads + head;
+    return v;
+  };
+  // Persistent grids: resident blocks per SM at the bucket's shared memory, and for L2-streamed buckets no more
+  // blocks than keep their states within 60% of L2 (the reference's ResidentBlocks rule, cc_pbils_gpu.cu:61-67).
+  std::string desc;
+  for (size_t i = 0; i < b.buckets.size(); ++i) {
+    ccb_batch::Bucket& bk = b.buckets[i];
+    size_t state = 0;
+    for (int m : bk.members) state = std::max(state, L2StateBytes(*b.inst[b.batched[m]].solver));
+    const int per_sm = BatchDescentBlocksPerSm(bk.shape);
+    long long grid = (long long)per_sm * b.device.sms;
+    if (state > 0) grid = std::min<long long>(grid, std::max<long long>(1, (long long)(0.6 * b.device.l2_bytes / state)));
+    bk.shape.grid = (int)std::max<long long>(1, std::min<long long>(grid, bk.total));
+    CCB_CUDA(LaunchBatchDescent(bk.shape, nullptr, BatchQueue{}, nullptr, true));
+    CCB_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
+    CCB_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
+    char line[160];
+    std::snprintf(line, sizeof(line), "%s k=%d threads=%d vpt=%d smem=%d: %zu instances, %d slots, grid %d; ",
+                  bk.shape.kind == kBatchRegisters ? "registers" : (bk.shape.kind == kBatchStream ? "stream" : "incremental"),
+                  bk.shape.k, bk.shape.threads, bk.shape.vpt, (int)bk.shape.smem, bk.members.size(), bk.total, bk.shape.grid);
+    desc += line;
+  }
+  b.rebuild_queue = view(rebuild_at, queues.back(), (int)b.buckets.size());
+  b.rebuild_grid = std::max(1, std::min(2 * b.device.sms, b.rebuild_queue.total));
+  b.description = desc;
+  for (cudaEvent_t& e : b.poll) CCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+
+  // One PBILS iteration of every instance as a graph: descents (bucket kernels on parallel branches), record,
+  // rebuild with perturbation, advance.
+  if (count > 0) {
+    cudaEvent_t fork;
+    CCB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CCB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+    CCB_CUDA(cudaMemsetAsync(b.d_heads, 0, (b.buckets.size() + 1) * sizeof(int32_t), b.stream));
+    CCB_CUDA(cudaEventRecord(fork, b.stream));
+    for (size_t i = 0; i < b.buckets.size(); ++i) {
+      ccb_batch::Bucket& bk = b.buckets[i];
+      CCB_CUDA(cudaStreamWaitEvent(bk.stream, fork, 0));
+      CCB_CUDA(LaunchBatchDescent(bk.shape, b.d_entries, view(bk.offset, BatchQueue{nullptr, nullptr,
+                                  (int32_t)bk.members.size(), bk.total, nullptr}, (int)i), bk.stream, false));
+      CCB_CUDA(cudaEventRecord(bk.done, bk.stream));
+      CCB_CUDA(cudaStreamWaitEvent(b.stream, bk.done, 0));
+    }
+    CCB_CUDA(LaunchBatchRecord(b.d_entries, count, b.stream));
+    CCB_CUDA(LaunchBatchRebuild(b.d_entries, b.rebuild_queue, b.rebuild_grid, b.stream));
+    CCB_CUDA(cudaMemsetAsync(b.d_active, 0, sizeof(int32_t), b.stream));
+    CCB_CUDA(LaunchBatchAdvance(b.d_entries, count, b.d_active, b.stream));
+    CCB_CUDA(cudaStreamEndCapture(b.stream, &b.graph));
+    CCB_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
+    cudaEventDestroy(fork);
+  }
+  b.prepared = true;
+}
+
+// Initial population, rebuild and record of one instance (as RunPbils does before its loop).
+void EnqueueInit(ccb_solver& s, const ccb_params& p, cudaStream_t st) {
+  CCB_CUDA(cudaMemsetAsync(s.ctl, 0, sizeof(Control), st));
+  k_mark_start<<<1, 1, 0, st>>>(s.ctl);
+  const long long total = (long long)s.pop * s.n;
+  const int init_grid = (int)std::max<long long>(1, std::min<long long>(CeilDiv(total, kAuxThreads), 4096));
+  k_init_labels<<<init_grid, kAuxThreads, 0, st>>>(s.cur_lab, s.pop, s.n, s.ld, s.k, StreamSeed(p.seed, kInitTag, 0));
+  CCB_CUDA(cudaGetLastError());
+  LaunchRebuild<int16_t>(s, s.pop, kRebuildInPlace, nullptr, 0, 0, 0.f, 0, false, st);
+  RecordArgs r{};
+  r.f = s.cur_f;
+  r.labels = s.cur_lab;
+  r.ld = s.ld;
+  r.n = s.n;
+  r.count = s.pop;
+  r.ctl = s.ctl;
+  r.record_labels = s.record_lab;
+  r.mode = kRecordInitial;
+  LaunchRecord(s, r, st);
+  if (p.iterations <= 0) {
+    // nothing to iterate: mark the instance stopped before the first graph replay
+    const int one = 1;
+    CCB_CUDA(cudaMemcpyAsync(&s.ctl->stop, &one, sizeof(one), cudaMemcpyHostToDevice, st));
+  }
+}
+
+void RunBatch(ccb_batch& b) {
+  const auto started = std::chrono::steady_clock::now();
+  PrepareBatch(b);
+  const cudaStream_t st = b.stream;
+  for (int e = 0; e < (int)b.batched.size(); ++e) {
+    ccb_batch::Instance& in = b.inst[b.batched[e]];
+    EnqueueInit(*in.solver, in.params, st);
+  }
+  if (b.exec != nullptr) {
+    int chunk = 0;
+    for (int r = 0; r < b.max_iterations; ++r) {
+      CCB_CUDA(cudaGraphLaunch(b.exec, st));
+      ++b.replays;
+      if ((r + 1) % kPollChunk == 0 && r + 1 < b.max_iterations) {
+        const int slot = chunk % 2;
+        if (chunk >= 1) {
+          CCB_CUDA(cudaEventSynchronize(b.poll[1 - slot]));
+          if (b.h_active[1 - slot] == 0) break;
+        }
+        CCB_CUDA(cudaMemcpyAsync(&b.h_active[slot], b.d_active, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CCB_CUDA(cudaEventRecord(b.poll[slot], st));
+        ++chunk;
+      }
+    }
+  }
+  CCB_CUDA(cudaStreamSynchronize(st));
+  const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
+  for (size_t i = 0; i < b.inst.size(); ++i) {
+    ccb_batch::Instance& in = b.inst[i];
+    std::memset(&in.result, 0, sizeof(in.result));
+    in.labels.assign(in.graph->n, 0);
+    if (in.graph->n == 0) {
+      EmptyPbils(in.params, &in.result);
+      continue;
+    }
+    if (!in.batched) {
+      RunPbils<int16_t>(*in.solver, in.params, st, in.labels.data(), &in.result);
+      continue;
+    }
+    ccb_solver& s = *in.solver;
+    CopyOutLabels(s, in.labels.data(), st);
+    const Control& c = s.host_ctl[0];
+    if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+    in.result.objective = c.record_f;
+    in.result.iterations_done = c.iterations_done;
+    in.result.local_searches = (int64_t)c.iterations_done * s.pop;
+    in.result.accepted_moves = (int64_t)c.moves;
+    in.result.clusters_used = CountClustersUsed(in.labels.data(), (uint32_t)s.n, s.k);
+    in.result.seconds = seconds;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------------------
 extern "C" {
@@ -899,6 +1174,50 @@ int ccb_solver_stats(const ccb_solver* s, ccb_kernel_stats* stats) {
     *stats = s->stats;
   });
 }
+
+int ccb_batch_create(ccb_batch** out) {
+  return Guard([&] {
+    if (!out) Fail(CCB_ERR_STATE, "null output handle");
+    std::unique_ptr<ccb_batch> b(new ccb_batch());
+    b->device = Device::Current();
+    *out = b.release();
+  });
+}
+
+int ccb_batch_add(ccb_batch* b, const ccb_graph* g, const ccb_params* params, int32_t* id_out) {
+  return Guard([&] {
+    if (!b || !g || !params) Fail(CCB_ERR_STATE, "null argument");
+    if (b->prepared) Fail(CCB_ERR_STATE, "batch already prepared: create a new batch to add instances");
+    CheckParams(*params);
+    CheckGpuLimits(*params, (uint32_t)g->n);
+    ccb_batch::Instance in;
+    in.graph = g;
+    in.params = *params;
+    b->inst.push_back(std::move(in));
+    if (id_out) *id_out = (int32_t)b->inst.size() - 1;
+  });
+}
+
+int ccb_batch_run(ccb_batch* b) {
+  return Guard([&] {
+    if (!b) Fail(CCB_ERR_STATE, "null batch");
+    RunBatch(*b);
+  });
+}
+
+int ccb_batch_result(const ccb_batch* b, int32_t id, int32_t* labels_out, ccb_result* result) {
+  return Guard([&] {
+    if (!b || !result) Fail(CCB_ERR_STATE, "null argument");
+    if (id < 0 || id >= (int32_t)b->inst.size()) Fail(CCB_ERR_STATE, "no such instance");
+    const ccb_batch::Instance& in = b->inst[id];
+    *result = in.result;
+    if (labels_out && !in.labels.empty()) std::memcpy(labels_out, in.labels.data(), in.labels.size() * 4);
+  });
+}
+
+const char* ccb_batch_describe(const ccb_batch* b) { return b ? b->description.c_str() : ""; }
+
+void ccb_batch_destroy(ccb_batch* b) { delete b; }
 
 int ccb_pbils_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                     const ccb_params* params, int32_t* labels_out, ccb_result* result) {

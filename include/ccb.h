@@ -100,6 +100,15 @@ int ccb_graph_upload(const uint32_t* bits, uint32_t n, uint32_t words_per_row, u
 /* Same from a device bitset (e.g. a framework tensor); the library keeps its own copy. */
 int ccb_graph_from_device(const uint32_t* device_bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                           void* stream, ccb_graph** out);
+/* Graph::ErdosRenyi (src/cc_graph.cpp:168-177) generated on the device: the same bits as
+ * ccb_generate_erdos_renyi on the host, by closed-form jump-ahead of the splitmix64 stream. */
+int ccb_graph_generate_erdos_renyi(uint32_t n, double density, uint64_t seed, void* stream, ccb_graph** out);
+/* The planted partition of ccb_generate_planted, generated on the device (communities on the host).
+ * community_out (host, n entries) may be NULL.  No counterpart in the reference. */
+int ccb_graph_generate_planted(uint32_t n, int32_t parts, int32_t shuffle_split, double p_in, double p_out,
+                               double flip, uint64_t seed, void* stream, ccb_graph** out, int32_t* community_out);
+/* Copies a device graph back into the reference's host layout (n rows of words_per_row words). */
+int ccb_graph_download(const ccb_graph* graph, uint32_t* bits, uint32_t words_per_row);
 int ccb_graph_size(const ccb_graph* graph, uint32_t* n, uint64_t* edges);
 void ccb_graph_destroy(ccb_graph* graph);
 
@@ -131,6 +140,24 @@ typedef struct ccb_kernel_stats {
 } ccb_kernel_stats;
 int ccb_solver_set_profiling(ccb_solver* solver, int32_t enabled);
 int ccb_solver_stats(const ccb_solver* solver, ccb_kernel_stats* stats);
+
+/* ---- batched solves ----------------------------------------------------------------------------
+ * No counterpart in the reference (which solves one instance per call).  Many independent PBILS instances
+ * (each its own graph, k, population, seed, ...) run together: every iteration of all instances is one
+ * CUDA graph replay whose descent phase is a persistent kernel per shape bucket, draining a device queue of
+ * (instance, slot) work items; record, GWW and perturbation+rebuild follow as one kernel each.  Results
+ * are the same as ccb_solver_pbils / ccb_pbils_solve would give each instance alone, bit for bit.
+ * Graphs are device-resident (ccb_graph_upload) and must outlive the batch.  Instances with k = 1 or
+ * n > 32767 are solved one by one on the plain path after the batched ones. */
+typedef struct ccb_batch ccb_batch;
+int ccb_batch_create(ccb_batch** out);
+int ccb_batch_add(ccb_batch* batch, const ccb_graph* graph, const ccb_params* params, int32_t* id_out);
+/* Solves every instance (again on each call: same inputs, same results).  Synchronous. */
+int ccb_batch_run(ccb_batch* batch);
+int ccb_batch_result(const ccb_batch* batch, int32_t id, int32_t* labels_out, ccb_result* result);
+/* Text description of the buckets (kernel, shape, instances, slots, persistent grid). */
+const char* ccb_batch_describe(const ccb_batch* batch);
+void ccb_batch_destroy(ccb_batch* batch);
 
 /* ---- device recount -----------------------------------------------------------------------------
  * Objective f, cluster sizes and G = A*Z of `count` labelings of one graph, computed on the device:

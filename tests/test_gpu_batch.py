@@ -1,0 +1,71 @@
+"""Device graph generation and the batched engine.
+
+Generated graphs must equal the host generators bit for bit; every instance of a batch must give exactly
+the result of its plain solve (and of the CPU oracle where that is quick)."""
+import numpy as np
+import pytest
+
+from oracle import make_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 100, 1000, 3001])
+def test_device_erdos_renyi_matches_host(ccb, oracle, cuda_device, n):
+    for density in (0.0, 0.33, 1.0):
+        g = ccb.DeviceGraph.erdos_renyi(n, density, 7 + n).download()
+        bits, edges = oracle.erdos_renyi(n, density, 7 + n)
+        assert g.edges == edges and np.array_equal(g.bits, bits)
+
+
+@pytest.mark.parametrize("n,parts,split", [(64, 2, True), (1000, 5, False), (2500, 2, True), (33, 3, False)])
+def test_device_planted_matches_host(ccb, oracle, cuda_device, n, parts, split):
+    dg, comm = ccb.DeviceGraph.planted(n, parts, 0.6, 0.1, 0.07, 11, shuffle_split=split)
+    g = dg.download()
+    bits, edges, comm_o = oracle.planted(n, parts, split, 0.6, 0.1, 0.07, 11)
+    assert g.edges == edges and np.array_equal(g.bits, bits) and np.array_equal(comm, comm_o)
+
+
+MIX = [
+    # n, k, pop, gww, tournament, iterations, early_stop, perturbation, seed
+    (60, 2, 8, 0.1, 5, 6, 6, 0.4, 1),
+    (300, 5, 32, 0.25, 5, 10, 4, 0.4, 2),
+    (1000, 3, 64, 0.1, 3, 8, 100, 0.3, 3),
+    (1500, 8, 16, 0.0, 5, 5, 2, 0.4, 4),
+    (4500, 4, 8, 0.1, 5, 2, 6, 0.4, 5),
+    (700, 12, 32, 0.1, 5, 6, 6, 0.4, 6),
+    (2500, 33, 8, 0.5, 5, 3, 6, 0.4, 7),
+    (200, 64, 12, 0.1, 5, 4, 6, 0.4, 8),
+    (5, 2, 3, 0.0, 2, 0, 6, 0.4, 9),
+    (90, 1, 4, 0.1, 5, 3, 6, 0.4, 10),
+]
+
+
+def test_batch_matches_plain_and_oracle(ccb, oracle, cuda_device):
+    batch = ccb.Batch()
+    graphs, params, ids = [], [], []
+    for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(MIX):
+        dg, _ = ccb.DeviceGraph.planted(n, max(2, k // 2), 0.5, 0.05, 0.1, 100 + i)
+        p = ccb.PbilsParams(k=k, population=pop, gww=gww, tournament=tour, iterations=iters, early_stop=early,
+                            perturbation=pert, seed=seed)
+        graphs.append(dg)
+        params.append(p)
+        ids.append(batch.add(dg, p))
+    batch.run()
+    for i, (dg, p) in enumerate(zip(graphs, params)):
+        got = batch.result(ids[i])
+        host = dg.download()
+        want = ccb.SolveGpu(host, p)
+        assert (got.objective, got.iterations_done, got.accepted_moves, got.local_searches, got.clusters_used) == \
+            (want.objective, want.iterations_done, want.accepted_moves, want.local_searches, want.clusters_used), i
+        assert np.array_equal(got.labels, want.labels), i
+        if host.n <= 1500:
+            o = oracle.pbils(host.bits, host.edges, make_params(k=p.k, population=p.population, gww=p.gww,
+                                                                tournament=p.tournament, iterations=p.iterations,
+                                                                early_stop=p.early_stop,
+                                                                perturbation=p.perturbation, seed=p.seed))
+            assert o.objective == got.objective and np.array_equal(o.labels, got.labels), i
+    # a second run of the same batch reproduces every result
+    first = [batch.result(i).objective for i in ids]
+    batch.run()
+    assert [batch.result(i).objective for i in ids] == first
