@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import statistics
@@ -48,8 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=256, help="batched workload: instances")
+    ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
     return ap.parse_args()
 
 
@@ -177,11 +180,108 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def percentile(xs, q):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(math.ceil(q * len(xs))) - 1)] if xs else None
+
+
+def run_batched(args, rank, world, local):
+    """The batched mix (cuda_graph_clustering_b200.workloads.batched_mix, master seed 7 + rank): every
+    instance solved by the batched engine (all together, one graph replay per iteration) and by the plain
+    path (one ccb_solver_pbils call per instance, in order), on the same device-resident graphs; each
+    batched result is checked equal to its plain result.  Latencies are completion times of a FIFO in
+    which all instances arrive at once."""
+    import torch
+
+    import cuda_graph_clustering_b200 as ccb
+    from cuda_graph_clustering_b200.workloads import batched_mix
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    mix = batched_mix(args.batch_count, master=7 + rank, iterations=args.batch_iters)
+    graphs = [ccb.DeviceGraph.planted(i.n, i.parts, i.p_in, i.p_out, i.flip, i.graph_seed)[0] for i in mix]
+    params = [ccb.PbilsParams(k=i.k, population=i.population, iterations=i.iterations, early_stop=i.iterations,
+                              gww=0.1, seed=i.seed) for i in mix]
+    batch = ccb.Batch()
+    ids = [batch.add(g, p) for g, p in zip(graphs, params)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        batch.run()
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_batch = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        batch.run()
+        t_batch.append(time.perf_counter() - t0)
+    clock_info = clocks.stop()
+    got = [batch.result(i) for i in ids]
+
+    solvers = [ccb.Solver(g, p) for g, p in zip(graphs, params)]
+    for s_, p in list(zip(solvers, params))[:8]:
+        s_.pbils(p, want_labels=False)
+    torch.cuda.synchronize()
+    t_plain = []
+    exact = True
+    for s_, p, r in zip(solvers, params, got):
+        t0 = time.perf_counter()
+        w = s_.pbils(p)
+        t_plain.append(time.perf_counter() - t0)
+        exact &= (w.objective == r.objective and w.iterations_done == r.iterations_done
+                  and w.accepted_moves == r.accepted_moves and bool((w.labels == r.labels).all()))
+    barrier()
+    tb = max(t_batch)
+    tp = sum(t_plain)
+    vals = torch.tensor([tb, tp], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    tb_all, tp_all = vals[0].item(), vals[1].item()
+    if rank == 0:
+        count = len(mix)
+        done = []
+        acc = 0.0
+        for t in t_plain:
+            acc += t
+            done.append(acc)
+        line = {
+            "metric": "batched solves/s", "value": world * count / tb_all, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tb_all, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "config": {"workload": f"batched mix: {count} planted instances, n log-uniform [200, 20000], k 2..64, "
+                                   f"pop {{32, 64, 128}}, {args.batch_iters} iterations, gww 0.1, master seed 7 + rank",
+                       "parallelism": f"replicas x{world}", "buckets": batch.describe()},
+            "plain_solves_per_s": world * count / tp_all,
+            "speedup_vs_plain": tp_all / tb_all,
+            "latency_s": {"batched_p50": tb, "batched_p99": tb, "plain_fifo_p50": percentile(done, 0.5),
+                          "plain_fifo_p99": percentile(done, 0.99)},
+            "bit_exact_vs_plain": bool(exact),
+            "clocks": clock_info,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "batched":
+        run_batched(args, rank, world, local)
         return
 
     import numpy as np
