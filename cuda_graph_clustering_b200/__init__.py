@@ -321,3 +321,82 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """A request loop with continuous batching (ccb_server_*): submitted requests queue FIFO, are admitted
+    while their device memory fits the budget, advance one PBILS iteration per step together with every
+    other admitted request, and retire when they finish.  Each result equals the request's plain solve."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_active: int = 0):
+        h = C.c_void_p()
+        check(lib().ccb_server_create(hbm_budget_bytes, max_active, C.byref(h)))
+        self.handle = h
+        self.sizes = {}
+        self._ids = (C.c_int32 * 4096)()
+
+    def submit(self, graph: Graph, params: PbilsParams) -> int:
+        p = params.to_c()
+        i = C.c_int32()
+        bits = np.ascontiguousarray(graph.bits, dtype=np.uint32)
+        check(lib().ccb_server_submit(self.handle, bits.ctypes.data if graph.n else None, graph.n,
+                                      graph.WordsPerRow(), graph.edges, C.byref(p), C.byref(i)))
+        self.sizes[int(i.value)] = graph.n
+        return int(i.value)
+
+    def submit_generated(self, params: PbilsParams, n: int, density: float = 0.0, seed: int = 0,
+                         planted: bool = False, parts: int = 2, p_in: float = 0.0, p_out: float = 0.0,
+                         flip: float = 0.0) -> int:
+        """A request whose graph is generated on the device at admission: Erdős–Rényi(n, density, seed), or
+        with planted=True the planted partition(n, parts, p_in, p_out, flip, seed)."""
+        p = params.to_c()
+        i = C.c_int32()
+        check(lib().ccb_server_submit_generated(self.handle, 1 if planted else 0, n, p_in if planted else density,
+                                                p_out, flip, parts, seed, C.byref(p), C.byref(i)))
+        self.sizes[int(i.value)] = n
+        return int(i.value)
+
+    def step(self) -> list:
+        """Admission, one iteration of every active request, retirement; returns the ids finished."""
+        count = C.c_int32()
+        check(lib().ccb_server_step(self.handle, self._ids, len(self._ids), C.byref(count)))
+        return [int(self._ids[j]) for j in range(min(count.value, len(self._ids)))]
+
+    def status(self) -> tuple:
+        """(queued, active, device bytes held by active requests)."""
+        q, a, b = C.c_int32(), C.c_int32(), C.c_uint64()
+        check(lib().ccb_server_status(self.handle, C.byref(q), C.byref(a), C.byref(b)))
+        return int(q.value), int(a.value), int(b.value)
+
+    def result(self, i: int) -> PbilsResult | None:
+        """The finished request's result (released from the server), or None while it runs."""
+        n = self.sizes[i]
+        labels = np.zeros(max(n, 1), np.int32)
+        res = CcbResult()
+        done = C.c_int32()
+        check(lib().ccb_server_result(self.handle, i, C.byref(done), labels.ctypes.data, C.byref(res)))
+        if not done.value:
+            return None
+        del self.sizes[i]
+        return PbilsResult.from_c(res, labels[:n])
+
+    def drain(self) -> dict:
+        """Steps until no request is queued or active; returns {id: result} for every request finished."""
+        out = {}
+        while True:
+            for i in self.step():
+                out[i] = self.result(i)
+            q, a, _ = self.status()
+            if q == 0 and a == 0:
+                return out
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ccb_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

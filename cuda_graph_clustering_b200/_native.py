@@ -75,6 +75,15 @@ SIGNATURES = {
     "ccb_batch_result": (C.c_int, [_vp, C.c_int32, _vp, C.POINTER(CcbResult)]),
     "ccb_batch_describe": (C.c_char_p, [_vp]),
     "ccb_batch_destroy": (None, [_vp]),
+    "ccb_server_create": (C.c_int, [C.c_uint64, C.c_int32, C.POINTER(_vp)]),
+    "ccb_server_submit": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(CcbParams),
+                                    C.POINTER(C.c_int32)]),
+    "ccb_server_submit_generated": (C.c_int, [_vp, C.c_int32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                              C.c_int32, C.c_uint64, C.POINTER(CcbParams), C.POINTER(C.c_int32)]),
+    "ccb_server_step": (C.c_int, [_vp, _i32p, C.c_int32, C.POINTER(C.c_int32)]),
+    "ccb_server_status": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
+    "ccb_server_result": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), _vp, C.POINTER(CcbResult)]),
+    "ccb_server_destroy": (None, [_vp]),
     "ccb_evaluate_labelings": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, _vp, _vp,
                                          _vp, _vp, _vp]),
     "ccb_evaluate_labelings_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32,

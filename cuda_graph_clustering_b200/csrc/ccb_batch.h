@@ -30,7 +30,7 @@ struct BatchQueue {
   int32_t* head;             // next unclaimed item (reset to 0 before every phase)
 };
 
-enum BatchKind : int { kBatchRegisters = 0, kBatchStream = 1, kBatchIncremental = 2 };
+enum BatchKind : int { kBatchRegisters = 0, kBatchStream = 1, kBatchIncremental = 2, kBatchIncrementalRegs = 3 };
 
 // Kernel instance of one descent bucket and its persistent grid.
 struct BatchShape {
@@ -49,7 +49,9 @@ cudaError_t LaunchBatchDescent(const BatchShape& shape, const BatchEntry* entrie
 int BatchDescentBlocksPerSm(const BatchShape& shape);
 cudaError_t LaunchBatchRebuild(const BatchEntry* entries, const BatchQueue& queue, int grid, cudaStream_t stream);
 cudaError_t LaunchBatchRecord(const BatchEntry* entries, int count, cudaStream_t stream);
-// Advances every running instance to its next iteration, stops those at their limit, counts the rest.
-cudaError_t LaunchBatchAdvance(const BatchEntry* entries, int count, int32_t* active, cudaStream_t stream);
+// Advances every running instance to its next iteration, stops those at their limit, counts the rest, and
+// (stops non-null) writes every instance's stop flag.
+cudaError_t LaunchBatchAdvance(const BatchEntry* entries, int count, int32_t* active, int32_t* stops,
+                               cudaStream_t stream);
 
 }  // namespace ccb

@@ -69,6 +69,17 @@ __global__ void __launch_bounds__(T, 1) kb_descent_incremental(const BatchEntry*
   }
 }
 
+template <int T, int V, bool S>
+__global__ void __launch_bounds__(T, 1) kb_descent_incremental_regs(const BatchEntry* __restrict__ entries,
+                                                                     BatchQueue q) {
+  __shared__ int s_item;
+  int entry, slot;
+  while (ClaimItem(q, &s_item, entry, slot)) {
+    DescentIncrementalRegs<T, V, S, (V >= 16)>(CurrentDescent(entries[entry]), slot);
+    __syncthreads();
+  }
+}
+
 constexpr int kBatchRebuildThreads = 512;
 
 __global__ void __launch_bounds__(kBatchRebuildThreads) kb_rebuild(const BatchEntry* __restrict__ entries,
@@ -91,23 +102,25 @@ __global__ void __launch_bounds__(kBatchRecordThreads) kb_record(const BatchEntr
   RecordBody<kBatchRecordThreads>(a);
 }
 
-__global__ void kb_advance(const BatchEntry* __restrict__ entries, int count, int32_t* active) {
+__global__ void kb_advance(const BatchEntry* __restrict__ entries, int count, int32_t* active, int32_t* stops) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   Control* c = entries[i].descent.ctl;
-  if (c->stop) return;
-  c->iter += 1;
-  if (c->iter >= entries[i].iterations) {
-    c->stop = 1;
-  } else {
-    atomicAdd(active, 1);
+  if (!c->stop) {
+    c->iter += 1;
+    if (c->iter >= entries[i].iterations) {
+      c->stop = 1;
+    } else {
+      atomicAdd(active, 1);
+    }
   }
+  if (stops != nullptr) stops[i] = c->stop;
 }
 
 template <typename Kernel>
 cudaError_t Run(Kernel kernel, const BatchShape& s, const BatchEntry* e, const BatchQueue& q, cudaStream_t st,
                 bool configure) {
-  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem_bytes);
+  if (configure) return RaiseDynamicSmem(kernel, s.smem_bytes);
   if (q.total == 0 || s.grid <= 0) return cudaSuccess;
   kernel<<<s.grid, s.threads, s.smem_bytes, st>>>(e, q);
   return cudaGetLastError();
@@ -134,6 +147,14 @@ cudaError_t WithKernel(const BatchShape& s, F&& f) {
   if (s.kind == kBatchStream && s.k == K) return s.smem ? f(kb_descent_stream<K, 1024, true>) : f(kb_descent_stream<K, 1024, false>);
   CCB_STREAM(2) CCB_STREAM(3) CCB_STREAM(4) CCB_STREAM(5) CCB_STREAM(6) CCB_STREAM(7) CCB_STREAM(8)
 #undef CCB_STREAM
+  if (s.kind == kBatchIncrementalRegs) {
+#define CCB_INC(T, V) \
+  if (s.threads == T && s.vpt == V) \
+    return s.smem ? f(kb_descent_incremental_regs<T, V, true>) : f(kb_descent_incremental_regs<T, V, false>);
+    CCB_INC(256, 4) CCB_INC(512, 4) CCB_INC(512, 8) CCB_INC(512, 16) CCB_INC(512, 32)
+#undef CCB_INC
+    return cudaErrorInvalidValue;
+  }
   if (s.kind == kBatchIncremental) {
     switch (s.threads) {
       case 256: return s.smem ? f(kb_descent_incremental<256, true>) : f(kb_descent_incremental<256, false>);
@@ -154,7 +175,7 @@ cudaError_t LaunchBatchDescent(const BatchShape& shape, const BatchEntry* entrie
 int BatchDescentBlocksPerSm(const BatchShape& shape) {
   int blocks = 1;
   WithKernel(shape, [&](auto kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape.smem_bytes);
+    RaiseDynamicSmem(kernel, shape.smem_bytes);
     blocks = Occupancy(kernel, shape);
     return cudaSuccess;
   });
@@ -173,9 +194,10 @@ cudaError_t LaunchBatchRecord(const BatchEntry* entries, int count, cudaStream_t
   return cudaGetLastError();
 }
 
-cudaError_t LaunchBatchAdvance(const BatchEntry* entries, int count, int32_t* active, cudaStream_t stream) {
+cudaError_t LaunchBatchAdvance(const BatchEntry* entries, int count, int32_t* active, int32_t* stops,
+                               cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
-  kb_advance<<<(count + 255) / 256, 256, 0, stream>>>(entries, count, active);
+  kb_advance<<<(count + 255) / 256, 256, 0, stream>>>(entries, count, active, stops);
   return cudaGetLastError();
 }
 

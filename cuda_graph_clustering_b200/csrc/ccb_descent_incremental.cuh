@@ -9,9 +9,13 @@
 //   lab[u]    the label a(u);
 //   kbest[u]  min over c != a(u) of key_c(u);   kown[u] = key_a(u)(u).
 // A move (v: from -> to) changes, for every u, only key_from and key_to (and G_from, G_to of neighbours of v).
-// So the cached minimum is updated from those two keys, and all K lanes are rescanned only when the cached
-// best target is `from` or `to` and its key grew (on average about one vertex in K - 1), or for v itself,
-// whose set of foreign clusters changed.  The update is folded into the next move's scan.
+// So the cached minimum is updated from those two keys; with a lower bound on the second-best key also
+// cached, all K lanes are rescanned only when the best known key reaches that bound, or for v itself, whose
+// set of foreign clusters changed.
+// Empty clusters are kept out of the per-vertex caches: an empty cluster's key is its index for every vertex,
+// so the best empty target is the lowest empty cluster, one value per block (with k far above the number of
+// communities, most vertices' best target is empty, and a cluster filling up would otherwise send them all
+// to rescan).  The update is folded into the next move's scan.
 #pragma once
 
 #include <cstdint>
@@ -20,31 +24,95 @@
 
 namespace ccb {
 
-// Smallest key over c != own of vertex u; the counters are cluster-major with leading dimension ld.
-__device__ __forceinline__ int RescanBest(const uint16_t* g, int ld, int u, const int* off, int k, int own) {
-  int best = 0x7fffffff;
+// Smallest and second smallest key over the non-empty clusters c != own of vertex u (off[c] >= 64 iff
+// size_c >= 1); the counters are cluster-major with leading dimension ld.  INT_MAX where there is none.
+__device__ __forceinline__ int2 RescanBest2(const uint16_t* g, int ld, int u, const int* off, int k, int own) {
+  int b1 = 0x7fffffff, b2 = 0x7fffffff;
+#pragma unroll 8
   for (int c = 0; c < k; ++c) {
-    const int key = off[c] - 128 * static_cast<int>(g[static_cast<size_t>(c) * ld + u]);
-    if (c != own) best = min(best, key);
+    const int o = off[c];
+    const int key = o - 128 * static_cast<int>(g[static_cast<size_t>(c) * ld + u]);
+    if (c != own && o >= 64) {
+      b2 = min(b2, max(b1, key));
+      b1 = min(b1, key);
+    }
   }
-  return best;
+  return make_int2(b1, b2);
 }
 
+__device__ __forceinline__ int RescanBest(const uint16_t* g, int ld, int u, const int* off, int k, int own) {
+  return RescanBest2(g, ld, u, off, k, own).x;
+}
+
+// Lowest-index empty cluster from a warp's off[] row, or -1.  An empty cluster c has size 0 and no
+// neighbours of any vertex in it, so its key is just c for every vertex: among empty targets the lowest
+// index always wins, and it is the same for all vertices.
+__device__ __forceinline__ int LowestEmpty(const int* off, int k) {
+  const int lane = threadIdx.x % kWarp;
+  const unsigned lo = __ballot_sync(kAllLanes, lane < k && off[lane] == lane);
+  const unsigned hi = __ballot_sync(kAllLanes, lane + 32 < k && off[lane + 32] == lane + 32);
+  return lo ? __ffs(lo) - 1 : (hi ? 32 + __ffs(hi) - 1 : -1);
+}
+
+// Folds the move (from -> to, `moved` = the vertex that moved) into the cached keys of vertex u, whose
+// counters G_from, G_to are already updated to gf, gt.  kb is the smallest key over the non-empty foreign
+// clusters, lb a lower bound on the second smallest, ko the key of u's own cluster (label = ko & 63).
+// Only key_from and key_to changed; every other foreign cluster but kb's is still >= lb.  So the best
+// known key is exact whenever it stays below lb, and all k lanes are rescanned only when it does not (the
+// cached best got worse than the bound) or for the moved vertex, whose foreign set changed.  After the move
+// `to` is non-empty; if `from` became empty it leaves the set.
+__device__ __forceinline__ void FoldMove(int u, int gf, int gt, int from, int to, int moved, bool from_empty,
+                                         const uint16_t* g, int ld, const int* off, int k, int& kb, int& lb,
+                                         int& ko) {
+  const int kf = off[from] - 128 * gf;
+  const int kt = off[to] - 128 * gt;
+  if (u == moved) {
+    ko = kt;
+    const int2 r = RescanBest2(g, ld, u, off, k, to);
+    kb = r.x;
+    lb = r.y;
+    return;
+  }
+  const int own = ko & 63;
+  if (own == from) ko = kf;
+  if (own == to) ko = kt;
+  const int b = kb == 0x7fffffff ? -1 : (kb & 63);
+  int m1 = (b == from || b == to) ? 0x7fffffff : kb;  // known keys: the cached best if unchanged,
+  int m2 = 0x7fffffff;
+  if (own != from && !from_empty) {                   // key_from if it is foreign and non-empty,
+    m2 = min(m2, max(m1, kf));
+    m1 = min(m1, kf);
+  }
+  if (own != to) {                                    // key_to if it is foreign
+    m2 = min(m2, max(m1, kt));
+    m1 = min(m1, kt);
+  }
+  if (m1 < lb) {
+    kb = m1;
+    lb = min(lb, m2);
+  } else {
+    const int2 r = RescanBest2(g, ld, u, off, k, own);
+    kb = r.x;
+    lb = r.y;
+  }
+}
 // Shared or global layout of one slot's incremental state (all arrays indexed by vertex, leading dimension ld).
 struct IncState {
   uint16_t* g;    // [k][ld] counters G_c(u), cluster-major: the two lanes a move touches are contiguous
   int* kbest;     // [ld]
   int* kown;      // [ld]
+  int* kbound;    // [ld] lower bound on the second-best foreign key
   uint8_t* lab;   // [ld]
 
   __host__ __device__ static size_t Bytes(int k, int ld) {
-    return static_cast<size_t>(ld) * (static_cast<size_t>(k) * 2 + 4 + 4 + 1);
+    return static_cast<size_t>(ld) * (static_cast<size_t>(k) * 2 + 4 + 4 + 4 + 1);
   }
   __device__ void Carve(unsigned char* base, int k, int ld) {
     g = reinterpret_cast<uint16_t*>(base);
     kbest = reinterpret_cast<int*>(base + static_cast<size_t>(k) * ld * 2);
     kown = kbest + ld;
-    lab = reinterpret_cast<uint8_t*>(kown + ld);
+    kbound = kown + ld;
+    lab = reinterpret_cast<uint8_t*>(kbound + ld);
   }
 };
 
@@ -99,7 +167,9 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
       const int own = l_src[u];
       st.lab[u] = static_cast<uint8_t>(own);
       st.kown[u] = off[own] - 128 * static_cast<int>(st.g[static_cast<size_t>(own) * ld + u]);
-      st.kbest[u] = RescanBest(st.g, ld, u, off, k, own);
+      const int2 r = RescanBest2(st.g, ld, u, off, k, own);
+      st.kbest[u] = r.x;
+      st.kbound[u] = r.y;
     }
   }
   long long objective = a.cur.f[w];
@@ -109,6 +179,8 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
   unsigned long long applied = 0;
   int parity = 0;
   int from = -1, to = -1, moved = -1;
+  bool from_empty = false;
+  int empty = LowestEmpty(off, k);
   const uint32_t* prev_row = nullptr;
   const uint32_t lane_bit = 1u << lane;
   const uint32_t key_base = (1u << bits) << bits;
@@ -117,7 +189,7 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
     uint32_t best = KeyTraits<uint32_t>::kNone;
     uint32_t payload = 0;
     for (int base = tid; base < n; base += U * T) {
-      int own[U], kb[U], ko[U];
+      int own[U], kb[U], ko[U], lbd[U];
       uint32_t rw[U];
 #pragma unroll
       for (int i = 0; i < U; ++i) {
@@ -126,6 +198,7 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
           own[i] = st.lab[u];
           kb[i] = st.kbest[u];
           ko[i] = st.kown[u];
+          lbd[i] = st.kbound[u];
           rw[i] = prev_row != nullptr ? prev_row[u >> 5] : 0u;
         }
       }
@@ -142,37 +215,20 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
             *g_from = static_cast<uint16_t>(--gf);
             *g_to = static_cast<uint16_t>(++gt);
           }
-          const int kf = off[from] - 128 * gf;
-          const int kt = off[to] - 128 * gt;
-          if (u == moved) {
-            // its own cluster changed: foreign set is new, rescan
-            own[i] = to;
-            st.lab[u] = static_cast<uint8_t>(to);
-            ko[i] = kt;
-            kb[i] = RescanBest(st.g, ld, u, off, k, to);
-          } else {
-            if (own[i] == from) ko[i] = kf;
-            if (own[i] == to) ko[i] = kt;
-            const int b = kb[i] & 63;
-            const bool from_foreign = own[i] != from;
-            const bool to_foreign = own[i] != to;
-            if ((b == from && kf > kb[i]) || (b == to && kt > kb[i])) {
-              kb[i] = RescanBest(st.g, ld, u, off, k, own[i]);
-            } else {
-              int m = (b == from || b == to) ? 0x7fffffff : kb[i];
-              if (from_foreign) m = min(m, kf);
-              if (to_foreign) m = min(m, kt);
-              kb[i] = m;
-            }
-          }
-          st.kbest[u] = kb[i];
-          st.kown[u] = ko[i];
+          const int kb0 = kb[i], ko0 = ko[i], lb0 = lbd[i];
+          FoldMove(u, gf, gt, from, to, moved, from_empty, st.g, ld, off, k, kb[i], lbd[i], ko[i]);
+          if (u == moved) st.lab[u] = static_cast<uint8_t>(to);
+          own[i] = ko[i] & 63;
+          if (kb[i] != kb0) st.kbest[u] = kb[i];
+          if (ko[i] != ko0) st.kown[u] = ko[i];
+          if (lbd[i] != lb0) st.kbound[u] = lbd[i];
         }
-        const int gain = (kb[i] >> 6) - (ko[i] >> 6) + 1;
+        const int kbest = min(kb[i], empty >= 0 ? empty : 0x7fffffff);
+        const int gain = (kbest >> 6) - (ko[i] >> 6) + 1;
         const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
         if (mk < best) {
           best = mk;
-          payload = static_cast<uint32_t>(own[i]) | (static_cast<uint32_t>(kb[i] & 63) << 8);
+          payload = static_cast<uint32_t>(own[i]) | (static_cast<uint32_t>(kbest & 63) << 8);
         }
       }
     }
@@ -188,6 +244,8 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
       off[to] += 64;
     }
     __syncwarp();
+    from_empty = off[from] == from;
+    empty = LowestEmpty(off, k);
     prev_row = a.gr.bits + static_cast<size_t>(moved) * pitch;
     objective += MoveDelta(m.key, bits);
     ++applied;
@@ -209,6 +267,199 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
 template <int T, bool kSmemState>
 __global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_t> a) {
   DescentIncremental<T, kSmemState>(a, blockIdx.x);
+}
+
+// The same descent with the cached keys owned per thread: thread t owns vertices u = t + j T, j < V
+// (n <= V T), and holds kbest, the second-best bound and kown of each (the label is kown & 63), in registers,
+// or for V >= 16 in [V][T] shared-memory arrays that only their owner touches (read eight at a time).  A move then costs, per owned vertex, the two
+// counter lanes `from` and `to` (one 16-bit load each, all of a thread's loads issued together) and the
+// adjacency word; the counters stay in shared memory when k * n * 2 bytes fit, else in the slot's rows of
+// `next` (L2).
+template <int T, int V, bool kSmemG, bool kSmemKeys>
+__device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t>& a, int slot) {
+  constexpr int kWarps = T / kWarp;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_winner;
+  __shared__ int s_stop;
+  __shared__ MoveRecord<uint32_t> s_records[2 * kWarps];
+  __shared__ int s_off[kWarps][kMaxK];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = a.gr.n;
+  const int k = a.k;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+  const int pitch = a.gr.pitch;
+
+  if (tid == 0) {
+    s_stop = a.ctl->stop;
+    if (!s_stop) {
+      const int64_t* f = a.cur.f;
+      s_winner = a.tournament > 0 ? TournamentWinner(a.select_stream, slot, a.iteration, a.population, a.tournament,
+                                                     [f](int i) { return f[i]; })
+                                  : slot;
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const int w = s_winner;
+
+  // dynamic shared memory: [cached keys: best, bound, own, each V x T ints, when kSmemKeys] [counters when kSmemG]
+  int* skb = reinterpret_cast<int*>(smem);
+  int* slb = skb + V * T;
+  int* sko = slb + V * T;
+  unsigned char* after_keys = smem + (kSmemKeys ? static_cast<size_t>(V) * T * 3 * sizeof(int) : 0);
+  uint16_t* g = kSmemG ? reinterpret_cast<uint16_t*>(after_keys)
+                       : reinterpret_cast<uint16_t*>(a.next.g) + static_cast<size_t>(slot) * k * ld;
+  int* off = s_off[warp];
+  const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+  for (int c = lane; c < kMaxK; c += kWarp) off[c] = c < k ? 64 * sizes[c] + c : 0x3fffffff;
+  __syncwarp();
+  {
+    const uint4* g_src = reinterpret_cast<const uint4*>(a.cur.g + static_cast<size_t>(w) * k * ld);
+    uint4* g_dst = reinterpret_cast<uint4*>(g);
+    for (size_t i = tid; i < static_cast<size_t>(k) * ld / 8; i += T) g_dst[i] = g_src[i];
+  }
+  __syncthreads();
+  constexpr int VR = kSmemKeys ? 1 : V;  // cached keys held in registers
+  int kb[VR], ko[VR], lbr[VR];
+  unsigned valid = 0;
+  {
+    const uint8_t* l_src = a.cur.labels + static_cast<size_t>(w) * ld;
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int u = tid + j * T;
+      int2 b = make_int2(0, 0);
+      int o = 0;
+      if (u < n) {
+        valid |= 1u << j;
+        const int own = l_src[u];
+        o = off[own] - 128 * static_cast<int>(g[static_cast<size_t>(own) * ld + u]);
+        b = RescanBest2(g, ld, u, off, k, own);
+      }
+      if constexpr (kSmemKeys) {
+        skb[j * T + tid] = b.x;
+        slb[j * T + tid] = b.y;
+        sko[j * T + tid] = o;
+      } else {
+        kb[j] = b.x;
+        lbr[j] = b.y;
+        ko[j] = o;
+      }
+    }
+  }
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+
+  unsigned long long applied = 0;
+  int parity = 0;
+  int from = 0, to = 0, moved = -1;
+  bool pending = false;
+  bool from_empty = false;
+  int empty = LowestEmpty(off, k);
+  const uint32_t* prev_row = a.gr.bits;
+  const uint32_t lane_bit = 1u << lane;
+  const uint32_t key_base = (1u << bits) << bits;
+
+  constexpr int kGroup = V < 8 ? V : 8;  // vertices whose loads are in flight together
+  while (true) {
+    uint32_t best = KeyTraits<uint32_t>::kNone;
+    uint32_t payload = 0;
+    // with the keys in shared memory nothing is indexed by j in registers: one group body, looped
+#pragma unroll(kSmemKeys ? 1 : V / kGroup)
+    for (int j0 = 0; j0 < V; j0 += kGroup) {
+      uint32_t rw[kGroup];
+      int gf[kGroup], gt[kGroup];
+#pragma unroll
+      for (int i = 0; i < kGroup; ++i) {
+        const int u = tid + (j0 + i) * T;
+        const bool live = pending && ((valid >> (j0 + i)) & 1);
+        rw[i] = live ? prev_row[u >> 5] : 0u;
+        gf[i] = live ? g[static_cast<size_t>(from) * ld + u] : 0;
+        gt[i] = live ? g[static_cast<size_t>(to) * ld + u] : 0;
+      }
+      int ckb[kGroup], clb[kGroup], cko[kGroup];
+      if constexpr (kSmemKeys) {
+#pragma unroll
+        for (int i = 0; i < kGroup; ++i) {
+          ckb[i] = skb[(j0 + i) * T + tid];
+          clb[i] = slb[(j0 + i) * T + tid];
+          cko[i] = sko[(j0 + i) * T + tid];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kGroup; ++i) {
+        const int j = j0 + i;
+        if (!((valid >> j) & 1)) continue;
+        const int u = tid + j * T;
+        int& kbj = kSmemKeys ? ckb[i] : kb[kSmemKeys ? 0 : j];
+        int& lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
+        int& koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
+        if (pending) {
+          if (rw[i] & lane_bit) {
+            g[static_cast<size_t>(from) * ld + u] = static_cast<uint16_t>(--gf[i]);
+            g[static_cast<size_t>(to) * ld + u] = static_cast<uint16_t>(++gt[i]);
+          }
+          const int kb0 = kbj, lb0 = lbj, ko0 = koj;
+          FoldMove(u, gf[i], gt[i], from, to, moved, from_empty, g, ld, off, k, kbj, lbj, koj);
+          if constexpr (kSmemKeys) {
+            if (kbj != kb0) skb[j * T + tid] = kbj;
+            if (lbj != lb0) slb[j * T + tid] = lbj;
+            if (koj != ko0) sko[j * T + tid] = koj;
+          }
+        }
+        const int kbest = min(kbj, empty >= 0 ? empty : 0x7fffffff);
+        const int gain = (kbest >> 6) - (koj >> 6) + 1;
+        const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
+        if (mk < best) {
+          best = mk;
+          payload = static_cast<uint32_t>(koj & 63) | (static_cast<uint32_t>(kbest & 63) << 8);
+        }
+      }
+    }
+    const MoveRecord<uint32_t> m = BlockArgMin<uint32_t, kWarps>(best, payload, s_records + parity * kWarps);
+    if (m.key >= key_base) break;
+    parity ^= 1;
+
+    moved = MoveVertex(m.key, bits);
+    from = static_cast<int>(m.payload & 0xff);
+    to = static_cast<int>(m.payload >> 8);
+    if (lane == 0) {
+      off[from] -= 64;
+      off[to] += 64;
+    }
+    __syncwarp();
+    from_empty = off[from] == from;
+    empty = LowestEmpty(off, k);
+    prev_row = a.gr.bits + static_cast<size_t>(moved) * pitch;
+    pending = true;
+    objective += MoveDelta(m.key, bits);
+    ++applied;
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      break;
+    }
+  }
+
+  uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    if ((valid >> j) & 1) {
+      const int o = kSmemKeys ? sko[j * T + tid] : ko[kSmemKeys ? 0 : j];
+      dst[tid + j * T] = static_cast<uint8_t>(o & 63);
+    }
+  }
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
+template <int T, int V, bool kSmemG, bool kSmemKeys>
+__global__ void __launch_bounds__(T, 1) k_descent_incremental_regs(DescentArgs<int16_t> a) {
+  DescentIncrementalRegs<T, V, kSmemG, kSmemKeys>(a, blockIdx.x);
 }
 
 }  // namespace ccb

@@ -13,7 +13,7 @@ namespace {
 template <int K, int T, bool S>
 cudaError_t GoStream(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
   auto kernel = k_descent_stream<K, T, S>;
-  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (configure) return RaiseDynamicSmem(kernel, smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -21,7 +21,7 @@ cudaError_t GoStream(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaS
 template <int K, int T, int V, bool R>
 cudaError_t GoRegisters(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
   auto kernel = k_descent_registers<K, T, V, R>;
-  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (configure) return RaiseDynamicSmem(kernel, smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -61,7 +61,7 @@ cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int 
 template <int T, bool S>
 cudaError_t GoIncremental(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
   auto kernel = k_descent_incremental<T, S>;
-  if (configure) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (configure) return RaiseDynamicSmem(kernel, smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -70,8 +70,43 @@ cudaError_t GoIncremental(const DescentArgs<int16_t>& a, int grid, size_t smem, 
 
 size_t IncrementalBytes(int k, int ld) { return IncState::Bytes(k, ld); }
 
+template <int T, int V, bool S>
+cudaError_t GoIncrementalRegs(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_incremental_regs<T, V, S, (V >= 16)>;
+  if (configure) return RaiseDynamicSmem(kernel, smem);
+  kernel<<<grid, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+size_t IncrementalRegsSmem(int k, int ld, int threads, int vpt, bool counters_in_smem) {
+  return (vpt >= 16 ? (size_t)vpt * threads * 12 : 0) + (counters_in_smem ? (size_t)k * ld * 2 : 0);
+}
+
+void IncrementalRegsShape(int n, int* threads, int* vpt) {
+  if (n <= 1024) {
+    *threads = 256, *vpt = 4;
+  } else if (n <= 2048) {
+    *threads = 512, *vpt = 4;
+  } else if (n <= 4096) {
+    *threads = 512, *vpt = 8;
+  } else if (n <= 8192) {
+    *threads = 512, *vpt = 16;
+  } else {
+    *threads = 512, *vpt = 32;
+  }
+}
+
 cudaError_t LaunchDescentIncremental(const SmallKPlan& p, const DescentArgs<int16_t>& a, int grid, cudaStream_t st,
                                      bool configure) {
+  if (p.registers) {
+#define CCB_INC(T, V)                                                                                     \
+  if (p.threads == T && p.vpt == V)                                                                       \
+    return p.smem_state ? GoIncrementalRegs<T, V, true>(a, grid, p.smem_bytes, st, configure)             \
+                        : GoIncrementalRegs<T, V, false>(a, grid, p.smem_bytes, st, configure);
+    CCB_INC(256, 4) CCB_INC(512, 4) CCB_INC(512, 8) CCB_INC(512, 16) CCB_INC(512, 32)
+#undef CCB_INC
+    return cudaErrorInvalidValue;
+  }
   switch (p.threads) {
     case 256:
       return p.smem_state ? GoIncremental<256, true>(a, grid, p.smem_bytes, st, configure)

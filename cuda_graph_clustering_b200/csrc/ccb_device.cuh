@@ -1,6 +1,8 @@
 // Device-side data views, control block and warp/block primitives of the PBILS pipeline.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "ccb_streams.cuh"
@@ -136,6 +138,17 @@ __device__ __forceinline__ long long BlockSum(long long v, long long* scratch) {
   for (int w = 0; w < kWarps; ++w) s += scratch[w];
   __syncthreads();
   return s;
+}
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`, never lowers it: several solvers (and
+// batches) share one kernel instance, each with its own need, so the limit must cover the largest.
+template <typename Kernel>
+inline cudaError_t RaiseDynamicSmem(Kernel kernel, size_t bytes) {
+  cudaFuncAttributes attr;
+  cudaError_t e = cudaFuncGetAttributes(&attr, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)attr.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 __device__ __forceinline__ int Bit(const uint32_t* row, int u) { return (row[u >> 5] >> (u & 31)) & 1; }

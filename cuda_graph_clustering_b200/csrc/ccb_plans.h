@@ -27,6 +27,10 @@ bool RegistersShapeBuilt(int threads, int vpt);
 // Incremental descent for 9 <= k <= 64 (ccb_descent_incremental.cuh): SmallKPlan fields threads,
 // smem_state and smem_bytes apply; k is the runtime cluster count.
 size_t IncrementalBytes(int k, int ld);
+// Threads and vertices per thread of the register-cached incremental form (n <= 16384).
+void IncrementalRegsShape(int n, int* threads, int* vpt);
+// Its dynamic shared memory: the cached keys (vpt >= 16) and, optionally, the counters.
+size_t IncrementalRegsSmem(int k, int ld, int threads, int vpt, bool counters_in_smem);
 cudaError_t LaunchDescentIncremental(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                      cudaStream_t stream, bool configure);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,

@@ -12,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
+#include <unordered_map>
 #include <memory>
 #include <tuple>
 #include <new>
@@ -232,9 +234,17 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
   if (!p.wide && k > 8 && ls_kernel == CCB_LS_AUTO) {
     SmallKPlan& sk = p.sk;
     sk.k = k;
-    sk.threads = n <= 2048 ? 256 : (n <= 8192 ? 512 : 1024);
-    sk.smem_state = IncrementalBytes(k, ld) + 10 * 1024 <= limit;  // the kernel's static shared memory
-    sk.smem_bytes = sk.smem_state ? IncrementalBytes(k, ld) : 0;
+    if (n <= 16384) {
+      // kbest / kown in registers, counters in shared memory when they fit
+      sk.registers = true;
+      IncrementalRegsShape(n, &sk.threads, &sk.vpt);
+      sk.smem_state = IncrementalRegsSmem(k, ld, sk.threads, sk.vpt, true) + 10 * 1024 <= limit;
+      sk.smem_bytes = IncrementalRegsSmem(k, ld, sk.threads, sk.vpt, sk.smem_state);
+    } else {
+      sk.threads = 1024;
+      sk.smem_state = IncrementalBytes(k, ld) + 10 * 1024 <= limit;  // the kernel's static shared memory
+      sk.smem_bytes = sk.smem_state ? IncrementalBytes(k, ld) : 0;
+    }
     p.incremental = true;
     p.smem_state = sk.smem_state;
     p.smem_rows = false;
@@ -248,7 +258,7 @@ template <typename GainT, typename Key, bool S, bool R, int T>
 void LaunchDescentT(const DescentArgs<GainT>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
   auto kernel = k_descent<GainT, Key, S, R, T>;
   if (configure) {
-    CCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CCB_CUDA(RaiseDynamicSmem(kernel, smem));
     return;
   }
   kernel<<<grid, T, smem, st>>>(a);
@@ -283,7 +293,13 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 }
 
 const char* KernelName(const Plan& p) {
-  if (p.incremental) return p.smem_state ? "incremental 9 <= k <= 64, shared memory" : "incremental 9 <= k <= 64, L2";
+  if (p.incremental) {
+    if (p.sk.registers) {
+      return p.smem_state ? "incremental 9 <= k <= 64, cached keys in registers, counters in shared memory"
+                          : "incremental 9 <= k <= 64, cached keys in registers, counters in L2";
+    }
+    return p.smem_state ? "incremental 9 <= k <= 64, shared memory" : "incremental 9 <= k <= 64, L2";
+  }
   if (p.small_k) {
     if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
                                            : "packed k <= 8, registers";
@@ -720,35 +736,59 @@ void CheckSolverMatches(const ccb_solver* s, const ccb_params& p) {
 // ------------------------------------------------------------------------------------------------
 // Batched engine: many instances, one CUDA graph per PBILS iteration, persistent bucket kernels
 // ------------------------------------------------------------------------------------------------
+// Device work lists of a set of instances (the batch or the server's active set): one descent bucket per
+// persistent kernel instance, plus the rebuild queue over all instances.
+struct WorkLists {
+  struct Bucket {
+    BatchShape shape;
+    std::vector<int> members;  // entry indices, heaviest first
+    int total = 0;
+    size_t offset = 0;         // of the member list in d_lists (int32 units)
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+  };
+  std::vector<Bucket> buckets;
+  BatchQueue rebuild{};
+  int rebuild_grid = 0;
+  int32_t* d_lists = nullptr;
+  size_t lists_cap = 0;
+  int32_t* d_heads = nullptr;  // one queue head per bucket + one for the rebuild queue
+  size_t heads_cap = 0;
+  cudaEvent_t fork = nullptr;
+  std::string description;
+
+  void ReleaseBuckets() {
+    for (Bucket& b : buckets) {
+      if (b.stream) cudaStreamDestroy(b.stream);
+      if (b.done) cudaEventDestroy(b.done);
+    }
+    buckets.clear();
+  }
+  ~WorkLists() {
+    ReleaseBuckets();
+    if (d_lists) cudaFree(d_lists);
+    if (d_heads) cudaFree(d_heads);
+    if (fork) cudaEventDestroy(fork);
+  }
+};
+
 struct ccb_batch {
   struct Instance {
     const ccb_graph* graph = nullptr;
     ccb_params params{};
     std::unique_ptr<ccb_solver> solver;
-    bool batched = false;  // false: solved on the plain path (k = 1, n = 0)
+    bool batched = false;  // false: solved on the plain path (k = 1, n = 0, n > 32767)
     ccb_result result{};
     std::vector<int32_t> labels;
   };
-  struct Bucket {
-    BatchShape shape;
-    std::vector<int> members;  // entry indices, heaviest first
-    int total = 0;
-    size_t offset = 0;         // of the member list in the device list buffer (int32 units)
-    cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
-  };
   Device device;
   std::vector<Instance> inst;
-  std::vector<Bucket> buckets;
   std::vector<int> entry_of;   // instance -> entry (-1 if not batched)
   std::vector<int> batched;    // entry -> instance
+  WorkLists work;
   BatchEntry* d_entries = nullptr;
-  int32_t* d_lists = nullptr;  // member lists and prefix sums of all queues
-  int32_t* d_heads = nullptr;  // one queue head per bucket + one for the rebuild queue
   int32_t* d_active = nullptr;
   int32_t* h_active = nullptr;  // pinned, two slots
-  BatchQueue rebuild_queue{};
-  int rebuild_grid = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t poll[2] = {nullptr, nullptr};
   cudaGraph_t graph = nullptr;
@@ -756,21 +796,15 @@ struct ccb_batch {
   bool prepared = false;
   int max_iterations = 0;
   long long replays = 0;
-  std::string description;
+  double l2_share = 0.0;  // 0: persistent grids fill every SM (see BuildWorkLists)
 
   ~ccb_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    for (Bucket& b : buckets) {
-      if (b.stream) cudaStreamDestroy(b.stream);
-      if (b.done) cudaEventDestroy(b.done);
-    }
     for (cudaEvent_t e : poll)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     if (d_entries) cudaFree(d_entries);
-    if (d_lists) cudaFree(d_lists);
-    if (d_heads) cudaFree(d_heads);
     if (d_active) cudaFree(d_active);
     if (h_active) cudaFreeHost(h_active);
   }
@@ -827,7 +861,7 @@ BatchShape ShapeOf(const ccb_solver& s) {
   sh.threads = sk.threads;
   sh.vpt = sk.vpt;
   if (s.plan.incremental) {
-    sh.kind = kBatchIncremental;
+    sh.kind = sk.registers ? kBatchIncrementalRegs : kBatchIncremental;
     sh.k = 0;
     sh.smem = sk.smem_state;
   } else if (sk.registers) {
@@ -843,9 +877,135 @@ BatchShape ShapeOf(const ccb_solver& s) {
 
 // Global-memory state bytes per running slot of an L2-streamed bucket (0 when the state is in shared memory).
 size_t L2StateBytes(const ccb_solver& s) {
-  if (s.plan.incremental) return s.plan.smem_state ? 0 : IncrementalBytes(s.k, s.ld);
+  if (s.plan.incremental) return s.plan.smem_state ? 0 : (s.plan.sk.registers ? (size_t)s.k * s.ld * 2
+                                                                                : IncrementalBytes(s.k, s.ld));
   if (!s.plan.sk.registers && !s.plan.smem_state) return (size_t)s.ld * SmallKLanes(s.k) * 2;
   return 0;
+}
+
+// Buckets, queues and persistent grids for the entries whose solvers are `solvers` (entry e = solvers[e]).
+// Persistent grids take the resident blocks per SM at the bucket's shared memory on every SM; with l2_share > 0
+// an L2-streamed bucket runs no more slots than keep their states within that share of L2 (the reference's
+// ResidentBlocks rule, cc_pbils_gpu.cu:61-67) -- off by default: on B200 the batched mix measured faster with
+// every SM busy.
+void BuildWorkLists(WorkLists& w, const std::vector<const ccb_solver*>& solvers, const Device& dev,
+                    double l2_share) {
+  w.ReleaseBuckets();
+  const int count = (int)solvers.size();
+  std::map<std::tuple<int, int, int, int, int>, int> index;
+  for (int e = 0; e < count; ++e) {
+    const BatchShape sh = ShapeOf(*solvers[e]);
+    const auto key = std::make_tuple(sh.kind, sh.k, sh.threads, sh.vpt, (int)sh.smem);
+    auto it = index.find(key);
+    if (it == index.end()) {
+      it = index.emplace(key, (int)w.buckets.size()).first;
+      w.buckets.emplace_back();
+      w.buckets.back().shape = sh;
+    }
+    WorkLists::Bucket& bk = w.buckets[it->second];
+    bk.shape.smem_bytes = std::max(bk.shape.smem_bytes, sh.smem_bytes);
+    bk.members.push_back(e);
+  }
+  std::vector<int32_t> lists;
+  auto add_queue = [&](std::vector<int>& members, BatchQueue& q) {
+    std::sort(members.begin(), members.end(),
+              [&](int x, int y) { return SlotWork(*solvers[x]) > SlotWork(*solvers[y]); });
+    const size_t at = lists.size();
+    for (int m : members) lists.push_back(m);
+    int total = 0;
+    for (int m : members) {
+      lists.push_back(total);
+      total += solvers[m]->pop;
+    }
+    lists.push_back(total);
+    q = BatchQueue{};
+    q.count = (int)members.size();
+    q.total = total;
+    return at;
+  };
+  std::vector<BatchQueue> queues(w.buckets.size());
+  for (size_t i = 0; i < w.buckets.size(); ++i) {
+    w.buckets[i].offset = add_queue(w.buckets[i].members, queues[i]);
+    w.buckets[i].total = queues[i].total;
+  }
+  std::vector<int> all(count);
+  for (int e = 0; e < count; ++e) all[e] = e;
+  BatchQueue rq{};
+  const size_t rebuild_at = add_queue(all, rq);
+  if (lists.size() > w.lists_cap) {
+    if (w.d_lists) cudaFree(w.d_lists);
+    w.lists_cap = std::max<size_t>(lists.size(), 2 * w.lists_cap);
+    CCB_CUDA(cudaMalloc(&w.d_lists, w.lists_cap * sizeof(int32_t)));
+  }
+  if (w.buckets.size() + 1 > w.heads_cap) {
+    if (w.d_heads) cudaFree(w.d_heads);
+    w.heads_cap = std::max<size_t>(w.buckets.size() + 1, 2 * w.heads_cap);
+    CCB_CUDA(cudaMalloc(&w.d_heads, w.heads_cap * sizeof(int32_t)));
+  }
+  if (!lists.empty()) {
+    CCB_CUDA(cudaMemcpy(w.d_lists, lists.data(), lists.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (w.fork == nullptr) CCB_CUDA(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
+  std::string desc;
+  for (size_t i = 0; i < w.buckets.size(); ++i) {
+    WorkLists::Bucket& bk = w.buckets[i];
+    size_t state = 0;
+    for (int m : bk.members) state = std::max(state, L2StateBytes(*solvers[m]));
+    const int per_sm = BatchDescentBlocksPerSm(bk.shape);
+    long long grid = (long long)per_sm * dev.sms;
+    if (state > 0 && l2_share > 0.0) {
+      grid = std::min<long long>(grid, std::max<long long>(1, (long long)(l2_share * dev.l2_bytes / state)));
+    }
+    bk.shape.grid = (int)std::max<long long>(1, std::min<long long>(grid, bk.total));
+    CCB_CUDA(LaunchBatchDescent(bk.shape, nullptr, BatchQueue{}, nullptr, true));
+    CCB_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
+    CCB_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
+    char line[160];
+    std::snprintf(line, sizeof(line), "%s k=%d threads=%d vpt=%d smem=%d: %zu instances, %d slots, grid %d; ",
+                  bk.shape.kind == kBatchRegisters          ? "registers"
+                  : bk.shape.kind == kBatchStream           ? "stream"
+                  : bk.shape.kind == kBatchIncrementalRegs  ? "incremental-registers"
+                                                            : "incremental",
+                  bk.shape.k, bk.shape.threads, bk.shape.vpt, (int)bk.shape.smem, bk.members.size(), bk.total,
+                  bk.shape.grid);
+    desc += line;
+    queues[i].instances = w.d_lists + bk.offset;
+    queues[i].prefix = w.d_lists + bk.offset + queues[i].count;
+    queues[i].head = w.d_heads + i;
+  }
+  rq.instances = w.d_lists + rebuild_at;
+  rq.prefix = w.d_lists + rebuild_at + rq.count;
+  rq.head = w.d_heads + w.buckets.size();
+  w.rebuild = rq;
+  w.rebuild_grid = std::max(1, std::min(2 * dev.sms, rq.total));
+  // bucket queue views are rebuilt from offsets at enqueue time
+  w.description = desc;
+}
+
+// One PBILS iteration of every entry: descents (bucket kernels on parallel streams), record, rebuild with
+// perturbation and GWW, advance.  `stops` (may be null) receives every entry's stop flag after the advance.
+void EnqueueIteration(WorkLists& w, const BatchEntry* d_entries, int count, int32_t* d_active, int32_t* d_stops,
+                      cudaStream_t st) {
+  if (count == 0) return;
+  CCB_CUDA(cudaMemsetAsync(w.d_heads, 0, (w.buckets.size() + 1) * sizeof(int32_t), st));
+  CCB_CUDA(cudaEventRecord(w.fork, st));
+  for (size_t i = 0; i < w.buckets.size(); ++i) {
+    WorkLists::Bucket& bk = w.buckets[i];
+    BatchQueue q{};
+    q.count = (int32_t)bk.members.size();
+    q.total = bk.total;
+    q.instances = w.d_lists + bk.offset;
+    q.prefix = w.d_lists + bk.offset + q.count;
+    q.head = w.d_heads + i;
+    CCB_CUDA(cudaStreamWaitEvent(bk.stream, w.fork, 0));
+    CCB_CUDA(LaunchBatchDescent(bk.shape, d_entries, q, bk.stream, false));
+    CCB_CUDA(cudaEventRecord(bk.done, bk.stream));
+    CCB_CUDA(cudaStreamWaitEvent(st, bk.done, 0));
+  }
+  CCB_CUDA(LaunchBatchRecord(d_entries, count, st));
+  CCB_CUDA(LaunchBatchRebuild(d_entries, w.rebuild, w.rebuild_grid, st));
+  CCB_CUDA(cudaMemsetAsync(d_active, 0, sizeof(int32_t), st));
+  CCB_CUDA(LaunchBatchAdvance(d_entries, count, d_active, d_stops, st));
 }
 
 void PrepareBatch(ccb_batch& b) {
@@ -854,6 +1014,7 @@ void PrepareBatch(ccb_batch& b) {
   b.entry_of.assign(b.inst.size(), -1);
   b.batched.clear();
   std::vector<BatchEntry> entries;
+  std::vector<const ccb_solver*> solvers;
   for (size_t i = 0; i < b.inst.size(); ++i) {
     ccb_batch::Instance& in = b.inst[i];
     if (in.graph->n == 0) continue;
@@ -864,120 +1025,24 @@ void PrepareBatch(ccb_batch& b) {
     b.entry_of[i] = (int)entries.size();
     b.batched.push_back((int)i);
     entries.push_back(MakeEntry(*in.solver, in.params));
+    solvers.push_back(in.solver.get());
     b.max_iterations = std::max(b.max_iterations, in.params.iterations);
   }
   const int count = (int)entries.size();
-  // Buckets: one persistent kernel instance each.
-  std::map<std::tuple<int, int, int, int, int>, int> index;
-  for (int e = 0; e < count; ++e) {
-    const ccb_solver& s = *b.inst[b.batched[e]].solver;
-    const BatchShape sh = ShapeOf(s);
-    const auto key = std::make_tuple(sh.kind, sh.k, sh.threads, sh.vpt, (int)sh.smem);
-    auto it = index.find(key);
-    if (it == index.end()) {
-      it = index.emplace(key, (int)b.buckets.size()).first;
-      b.buckets.emplace_back();
-      b.buckets.back().shape = sh;
-    }
-    ccb_batch::Bucket& bk = b.buckets[it->second];
-    bk.shape.smem_bytes = std::max(bk.shape.smem_bytes, sh.smem_bytes);
-    bk.members.push_back(e);
-  }
-  // Queue layout in one device buffer: per bucket members then prefix, then the rebuild queue.
-  std::vector<int32_t> lists;
-  std::vector<BatchQueue> queues;
-  auto add_queue = [&](std::vector<int>& members) {
-    std::sort(members.begin(), members.end(), [&](int x, int y) {
-      return SlotWork(*b.inst[b.batched[x]].solver) > SlotWork(*b.inst[b.batched[y]].solver);
-    });
-    BatchQueue q{};
-    const size_t at = lists.size();
-    for (int m : members) lists.push_back(m);
-    int total = 0;
-    for (int m : members) {
-      lists.push_back(total);
-      total += b.inst[b.batched[m]].solver->pop;
-    }
-    lists.push_back(total);
-    q.count = (int)members.size();
-    q.total = total;
-    queues.push_back(q);
-    return at;
-  };
-  for (ccb_batch::Bucket& bk : b.buckets) {
-    bk.offset = add_queue(bk.members);
-    bk.total = queues.back().total;
-  }
-  std::vector<int> all(count);
-  for (int e = 0; e < count; ++e) all[e] = e;
-  const size_t rebuild_at = add_queue(all);
-
+  BuildWorkLists(b.work, solvers, b.device, b.l2_share);
   CCB_CUDA(cudaMalloc(&b.d_entries, std::max<size_t>(1, entries.size()) * sizeof(BatchEntry)));
-  CCB_CUDA(cudaMalloc(&b.d_lists, std::max<size_t>(1, lists.size()) * sizeof(int32_t)));
-  CCB_CUDA(cudaMalloc(&b.d_heads, (b.buckets.size() + 1) * sizeof(int32_t)));
   CCB_CUDA(cudaMalloc(&b.d_active, sizeof(int32_t)));
   CCB_CUDA(cudaMallocHost(&b.h_active, 2 * sizeof(int32_t)));
   if (!entries.empty()) {
     CCB_CUDA(cudaMemcpy(b.d_entries, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice));
   }
-  if (!lists.empty()) {
-    CCB_CUDA(cudaMemcpy(b.d_lists, lists.data(), lists.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  }
-  auto view = [&](size_t at, const BatchQueue& q, int head) {
-    BatchQueue v = q;
-    v.instances = b.d_lists + at;
-    v.prefix = b.d_lists + at + q.count;
-    v.head = b.d_heads + head;
-    return v;
-  };
-  // Persistent grids: resident blocks per SM at the bucket's shared memory, and for L2-streamed buckets no more
-  // blocks than keep their states within 60% of L2 (the reference's ResidentBlocks rule, cc_pbils_gpu.cu:61-67).
-  std::string desc;
-  for (size_t i = 0; i < b.buckets.size(); ++i) {
-    ccb_batch::Bucket& bk = b.buckets[i];
-    size_t state = 0;
-    for (int m : bk.members) state = std::max(state, L2StateBytes(*b.inst[b.batched[m]].solver));
-    const int per_sm = BatchDescentBlocksPerSm(bk.shape);
-    long long grid = (long long)per_sm * b.device.sms;
-    if (state > 0) grid = std::min<long long>(grid, std::max<long long>(1, (long long)(0.6 * b.device.l2_bytes / state)));
-    bk.shape.grid = (int)std::max<long long>(1, std::min<long long>(grid, bk.total));
-    CCB_CUDA(LaunchBatchDescent(bk.shape, nullptr, BatchQueue{}, nullptr, true));
-    CCB_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
-    CCB_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
-    char line[160];
-    std::snprintf(line, sizeof(line), "%s k=%d threads=%d vpt=%d smem=%d: %zu instances, %d slots, grid %d; ",
-                  bk.shape.kind == kBatchRegisters ? "registers" : (bk.shape.kind == kBatchStream ? "stream" : "incremental"),
-                  bk.shape.k, bk.shape.threads, bk.shape.vpt, (int)bk.shape.smem, bk.members.size(), bk.total, bk.shape.grid);
-    desc += line;
-  }
-  b.rebuild_queue = view(rebuild_at, queues.back(), (int)b.buckets.size());
-  b.rebuild_grid = std::max(1, std::min(2 * b.device.sms, b.rebuild_queue.total));
-  b.description = desc;
   for (cudaEvent_t& e : b.poll) CCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-
-  // One PBILS iteration of every instance as a graph: descents (bucket kernels on parallel branches), record,
-  // rebuild with perturbation, advance.
+  // One PBILS iteration of every instance, captured once as a graph and replayed.
   if (count > 0) {
-    cudaEvent_t fork;
-    CCB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     CCB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
-    CCB_CUDA(cudaMemsetAsync(b.d_heads, 0, (b.buckets.size() + 1) * sizeof(int32_t), b.stream));
-    CCB_CUDA(cudaEventRecord(fork, b.stream));
-    for (size_t i = 0; i < b.buckets.size(); ++i) {
-      ccb_batch::Bucket& bk = b.buckets[i];
-      CCB_CUDA(cudaStreamWaitEvent(bk.stream, fork, 0));
-      CCB_CUDA(LaunchBatchDescent(bk.shape, b.d_entries, view(bk.offset, BatchQueue{nullptr, nullptr,
-                                  (int32_t)bk.members.size(), bk.total, nullptr}, (int)i), bk.stream, false));
-      CCB_CUDA(cudaEventRecord(bk.done, bk.stream));
-      CCB_CUDA(cudaStreamWaitEvent(b.stream, bk.done, 0));
-    }
-    CCB_CUDA(LaunchBatchRecord(b.d_entries, count, b.stream));
-    CCB_CUDA(LaunchBatchRebuild(b.d_entries, b.rebuild_queue, b.rebuild_grid, b.stream));
-    CCB_CUDA(cudaMemsetAsync(b.d_active, 0, sizeof(int32_t), b.stream));
-    CCB_CUDA(LaunchBatchAdvance(b.d_entries, count, b.d_active, b.stream));
+    EnqueueIteration(b.work, b.d_entries, count, b.d_active, nullptr, b.stream);
     CCB_CUDA(cudaStreamEndCapture(b.stream, &b.graph));
     CCB_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
-    cudaEventDestroy(fork);
   }
   b.prepared = true;
 }
@@ -1058,6 +1123,222 @@ void RunBatch(ccb_batch& b) {
     in.result.clusters_used = CountClustersUsed(in.labels.data(), (uint32_t)s.n, s.k);
     in.result.seconds = seconds;
   }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Serving engine: continuous batching at iteration granularity
+// ------------------------------------------------------------------------------------------------
+struct ccb_server {
+  struct Request {
+    int id = 0;
+    int source = 0;  // 0: host bitset, 1: Erdős–Rényi generated on the device, 2: planted generated on the device
+    std::vector<uint32_t> bits;
+    uint32_t n = 0, words = 0;
+    uint64_t edges = 0;
+    double density = 0, p_in = 0, p_out = 0, flip = 0;
+    int parts = 2;
+    uint64_t graph_seed = 0;
+    ccb_params params{};
+    size_t bytes = 0;  // device-memory estimate used for admission
+  };
+  struct Active {
+    Request req;
+    std::unique_ptr<ccb_graph> graph;
+    std::unique_ptr<ccb_solver> solver;
+    std::chrono::steady_clock::time_point admitted;
+  };
+  struct Done {
+    ccb_result result{};
+    std::vector<int32_t> labels;
+  };
+  Device device;
+  size_t budget = 0;
+  int max_active = 0;
+  size_t in_use = 0;
+  int next_id = 0;
+  std::deque<Request> queue;
+  std::vector<Active> active;  // entry order of the device table
+  std::unordered_map<int, Done> done;
+  WorkLists work;
+  BatchEntry* d_entries = nullptr;
+  size_t entries_cap = 0;
+  int32_t* d_active = nullptr;
+  int32_t* d_stops = nullptr;
+  int32_t* h_stops = nullptr;
+  size_t stops_cap = 0;
+  cudaStream_t stream = nullptr;
+  bool dirty = true;
+  long long steps = 0;
+
+  ~ccb_server() {
+    active.clear();
+    if (d_entries) cudaFree(d_entries);
+    if (d_active) cudaFree(d_active);
+    if (d_stops) cudaFree(d_stops);
+    if (h_stops) cudaFreeHost(h_stops);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// Device bytes of a request: its graph rows and degrees plus the solver's population buffers.
+size_t RequestBytes(const ccb_server& sv, uint32_t n, const ccb_params& p) {
+  const int words = (int)((n + 31) / 32);
+  const int pitch = std::max(4, (words + 3) / 4 * 4);
+  const size_t graph = (size_t)std::max<uint32_t>(n, 1) * pitch * 4 + (size_t)std::max<uint32_t>(n, 1) * 4;
+  const int ld = std::max(32, ((int)n + 31) / 32 * 32);
+  const int kpad = (p.k + 3) / 4 * 4;
+  const Plan plan = MakePlan((int)n, pitch, p.k, ld, kpad, CCB_LS_AUTO, sv.device);
+  const size_t labels = (size_t)p.population * ld;
+  const size_t gb = plan.wide ? 4 : 2;
+  const size_t next = plan.smem_state ? 0
+                      : plan.incremental ? (size_t)p.population * IncrementalBytes(p.k, ld)
+                                         : labels * (plan.small_k ? std::max(p.k, SmallKLanes(p.k)) : p.k) * gb;
+  return graph + 2 * labels + labels * p.k * gb + next + (size_t)p.population * kpad * 4 + 2 * (size_t)p.population * 8 +
+         (size_t)p.population * p.k * pitch * 4 + 2 * (size_t)p.population * 4 + ld + sizeof(Control);
+}
+
+void Finish(ccb_server& sv, ccb_server::Active& a, const ccb_result& r, std::vector<int32_t> labels) {
+  ccb_server::Done d;
+  d.result = r;
+  d.result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - a.admitted).count();
+  d.labels = std::move(labels);
+  sv.done[a.req.id] = std::move(d);
+}
+
+// Admits queued requests (FIFO) while the device-memory budget and the active-slot cap allow; a request
+// larger than the whole budget is admitted alone.  Requests the batched kernels do not take (n = 0, k = 1,
+// n > 32767) are solved on admission on the plain path.
+void Admit(ccb_server& sv) {
+  while (!sv.queue.empty() && (int)sv.active.size() < sv.max_active) {
+    ccb_server::Request& r = sv.queue.front();
+    if (sv.in_use + r.bytes > sv.budget && !sv.active.empty()) break;
+    ccb_server::Active a;
+    a.admitted = std::chrono::steady_clock::now();
+    a.req = std::move(r);
+    sv.queue.pop_front();
+    const ccb_server::Request& q = a.req;
+    if (q.source == 0) {
+      a.graph.reset(MakeGraph(q.bits.data(), false, q.n, q.words, q.edges, sv.stream));
+      a.req.bits.clear();
+      a.req.bits.shrink_to_fit();
+    } else {
+      ccb_graph* g = nullptr;
+      const int status =
+          q.source == 1 ? ccb_graph_generate_erdos_renyi(q.n, q.density, q.graph_seed, sv.stream, &g)
+                        : ccb_graph_generate_planted(q.n, q.parts, 0, q.p_in, q.p_out, q.flip, q.graph_seed, sv.stream,
+                                                     &g, nullptr);
+      if (status != CCB_OK) Fail(status, LastError());
+      a.graph.reset(g);
+    }
+    if (q.n == 0) {
+      ccb_result r0{};
+      EmptyPbils(q.params, &r0);
+      Finish(sv, a, r0, {});
+      continue;
+    }
+    a.solver.reset(MakeSolver(a.graph.get(), q.params.k, q.params.population, CCB_LS_AUTO));
+    const Plan& pl = a.solver->plan;
+    if (pl.wide || !(pl.small_k || pl.incremental)) {
+      std::vector<int32_t> labels(q.n);
+      ccb_result r0{};
+      if (pl.wide) {
+        RunPbils<int32_t>(*a.solver, q.params, sv.stream, labels.data(), &r0);
+      } else {
+        RunPbils<int16_t>(*a.solver, q.params, sv.stream, labels.data(), &r0);
+      }
+      Finish(sv, a, r0, std::move(labels));
+      continue;
+    }
+    EnqueueInit(*a.solver, q.params, sv.stream);
+    sv.in_use += q.bytes;
+    sv.active.push_back(std::move(a));
+    sv.dirty = true;
+  }
+}
+
+void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t* finished_count) {
+  const size_t done_before = sv.done.size();
+  std::vector<int> newly;
+  auto note = [&](int id) { newly.push_back(id); };
+  // ids finished on the plain path during admission
+  std::vector<int> before_ids;
+  before_ids.reserve(sv.done.size());
+  for (const auto& kv : sv.done) before_ids.push_back(kv.first);
+  Admit(sv);
+  if (sv.done.size() != done_before) {
+    std::sort(before_ids.begin(), before_ids.end());
+    for (const auto& kv : sv.done)
+      if (!std::binary_search(before_ids.begin(), before_ids.end(), kv.first)) note(kv.first);
+  }
+  const int count = (int)sv.active.size();
+  if (count > 0) {
+    if (sv.dirty) {
+      std::vector<BatchEntry> entries;
+      std::vector<const ccb_solver*> solvers;
+      for (ccb_server::Active& a : sv.active) {
+        entries.push_back(MakeEntry(*a.solver, a.req.params));
+        solvers.push_back(a.solver.get());
+      }
+      if ((size_t)count > sv.entries_cap) {
+        if (sv.d_entries) cudaFree(sv.d_entries);
+        if (sv.d_stops) cudaFree(sv.d_stops);
+        if (sv.h_stops) cudaFreeHost(sv.h_stops);
+        sv.entries_cap = std::max<size_t>(count, 2 * sv.entries_cap);
+        CCB_CUDA(cudaMalloc(&sv.d_entries, sv.entries_cap * sizeof(BatchEntry)));
+        CCB_CUDA(cudaMalloc(&sv.d_stops, sv.entries_cap * sizeof(int32_t)));
+        CCB_CUDA(cudaMallocHost(&sv.h_stops, sv.entries_cap * sizeof(int32_t)));
+      }
+      CCB_CUDA(cudaMemcpyAsync(sv.d_entries, entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
+                               sv.stream));
+      CCB_CUDA(cudaStreamSynchronize(sv.stream));
+      BuildWorkLists(sv.work, solvers, sv.device, 0.0);
+      sv.dirty = false;
+    }
+    EnqueueIteration(sv.work, sv.d_entries, count, sv.d_active, sv.d_stops, sv.stream);
+    CCB_CUDA(cudaMemcpyAsync(sv.h_stops, sv.d_stops, count * sizeof(int32_t), cudaMemcpyDeviceToHost, sv.stream));
+    CCB_CUDA(cudaStreamSynchronize(sv.stream));
+    ++sv.steps;
+    for (int e = count - 1; e >= 0; --e) {
+      if (!sv.h_stops[e]) continue;
+      ccb_server::Active& a = sv.active[e];
+      ccb_solver& s = *a.solver;
+      std::vector<int32_t> labels(s.n);
+      CopyOutLabels(s, labels.data(), sv.stream);
+      const Control& c = s.host_ctl[0];
+      if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+      ccb_result r{};
+      r.objective = c.record_f;
+      r.iterations_done = c.iterations_done;
+      r.local_searches = (int64_t)c.iterations_done * s.pop;
+      r.accepted_moves = (int64_t)c.moves;
+      r.clusters_used = CountClustersUsed(labels.data(), (uint32_t)s.n, s.k);
+      Finish(sv, a, r, std::move(labels));
+      note(a.req.id);
+      sv.in_use -= a.req.bytes;
+      sv.active.erase(sv.active.begin() + e);
+      sv.dirty = true;
+    }
+  }
+  if (finished_count) *finished_count = (int32_t)newly.size();
+  if (finished_ids) {
+    for (int i = 0; i < (int)newly.size() && i < capacity; ++i) finished_ids[i] = newly[i];
+  }
+}
+
+int Submit(ccb_server* sv, ccb_server::Request&& r, int32_t* id_out) {
+  return Guard([&] {
+    if (!sv) Fail(CCB_ERR_STATE, "null server");
+    CheckParams(r.params);
+    CheckGpuLimits(r.params, r.n);
+    r.id = sv->next_id++;
+    r.bytes = RequestBytes(*sv, r.n, r.params);
+    if (id_out) *id_out = r.id;
+    sv->queue.push_back(std::move(r));
+  });
 }
 
 }  // namespace
@@ -1215,9 +1496,89 @@ int ccb_batch_result(const ccb_batch* b, int32_t id, int32_t* labels_out, ccb_re
   });
 }
 
-const char* ccb_batch_describe(const ccb_batch* b) { return b ? b->description.c_str() : ""; }
+const char* ccb_batch_describe(const ccb_batch* b) { return b ? b->work.description.c_str() : ""; }
 
 void ccb_batch_destroy(ccb_batch* b) { delete b; }
+
+int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server** out) {
+  return Guard([&] {
+    if (!out) Fail(CCB_ERR_STATE, "null output handle");
+    std::unique_ptr<ccb_server> sv(new ccb_server());
+    sv->device = Device::Current();
+    size_t free_b = 0, total_b = 0;
+    CCB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    sv->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : free_b * 8 / 10;
+    sv->max_active = max_active > 0 ? max_active : 1024;
+    CCB_CUDA(cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking));
+    CCB_CUDA(cudaMalloc(&sv->d_active, sizeof(int32_t)));
+    *out = sv.release();
+  });
+}
+
+int ccb_server_submit(ccb_server* sv, const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                      const ccb_params* params, int32_t* id_out) {
+  if (!params) return Guard([] { Fail(CCB_ERR_STATE, "null argument"); });
+  ccb_server::Request r;
+  r.source = 0;
+  r.n = n;
+  r.words = words_per_row;
+  r.edges = edges;
+  r.params = *params;
+  if (n > 0) {
+    if (!bits || words_per_row < (n + 31) / 32) return Guard([] { Fail(CCB_ERR_INVALID, "bad bitset"); });
+    r.bits.assign(bits, bits + (size_t)n * words_per_row);
+  }
+  return Submit(sv, std::move(r), id_out);
+}
+
+int ccb_server_submit_generated(ccb_server* sv, int32_t planted, uint32_t n, double density_or_p_in, double p_out,
+                                double flip, int32_t parts, uint64_t graph_seed, const ccb_params* params,
+                                int32_t* id_out) {
+  if (!params) return Guard([] { Fail(CCB_ERR_STATE, "null argument"); });
+  ccb_server::Request r;
+  r.source = planted ? 2 : 1;
+  r.n = n;
+  r.density = density_or_p_in;
+  r.p_in = density_or_p_in;
+  r.p_out = p_out;
+  r.flip = flip;
+  r.parts = parts;
+  r.graph_seed = graph_seed;
+  r.params = *params;
+  return Submit(sv, std::move(r), id_out);
+}
+
+int ccb_server_step(ccb_server* sv, int32_t* finished_ids, int32_t capacity, int32_t* finished_count) {
+  return Guard([&] {
+    if (!sv) Fail(CCB_ERR_STATE, "null server");
+    ServerStep(*sv, finished_ids, capacity, finished_count);
+  });
+}
+
+int ccb_server_status(const ccb_server* sv, int32_t* queued, int32_t* active, uint64_t* bytes_in_use) {
+  return Guard([&] {
+    if (!sv) Fail(CCB_ERR_STATE, "null server");
+    if (queued) *queued = (int32_t)sv->queue.size();
+    if (active) *active = (int32_t)sv->active.size();
+    if (bytes_in_use) *bytes_in_use = (uint64_t)sv->in_use;
+  });
+}
+
+int ccb_server_result(ccb_server* sv, int32_t id, int32_t* done, int32_t* labels_out, ccb_result* result) {
+  return Guard([&] {
+    if (!sv || !done) Fail(CCB_ERR_STATE, "null argument");
+    auto it = sv->done.find(id);
+    *done = it != sv->done.end();
+    if (it == sv->done.end()) return;
+    if (result) *result = it->second.result;
+    if (labels_out && !it->second.labels.empty()) {
+      std::memcpy(labels_out, it->second.labels.data(), it->second.labels.size() * 4);
+    }
+    sv->done.erase(it);
+  });
+}
+
+void ccb_server_destroy(ccb_server* sv) { delete sv; }
 
 int ccb_pbils_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                     const ccb_params* params, int32_t* labels_out, ccb_result* result) {

@@ -159,6 +159,33 @@ int ccb_batch_result(const ccb_batch* batch, int32_t id, int32_t* labels_out, cc
 const char* ccb_batch_describe(const ccb_batch* batch);
 void ccb_batch_destroy(ccb_batch* batch);
 
+/* ---- serving ------------------------------------------------------------------------------------
+ * No counterpart in the reference.  A request loop with continuous batching: submitted requests wait in a
+ * FIFO queue; every ccb_server_step admits queued requests while their estimated device memory (graph rows
+ * + population buffers) fits the budget, runs ONE PBILS iteration for every admitted request together (the
+ * batched bucket kernels; each request keeps its own iteration count, so requests admitted at different
+ * steps interleave on the device), and retires the finished ones, freeing their memory for the queue.
+ * Each result equals the request's plain solve.  Requests the batched kernels do not take (k = 1,
+ * n > 32767) are solved on the plain path when admitted.  Not thread-safe: one host thread drives a server. */
+typedef struct ccb_server ccb_server;
+/* hbm_budget_bytes 0: 80% of the free device memory; max_active 0: 1024. */
+int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server** out);
+/* A request with a host bitset (copied at submission, uploaded at admission). */
+int ccb_server_submit(ccb_server* server, const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                      const ccb_params* params, int32_t* id_out);
+/* A request whose graph the server generates on the device at admission: Erdős–Rényi (planted = 0,
+ * density_or_p_in = density) or the planted partition (planted = 1, `parts` communities, p_in, p_out, flip). */
+int ccb_server_submit_generated(ccb_server* server, int32_t planted, uint32_t n, double density_or_p_in,
+                                double p_out, double flip, int32_t parts, uint64_t graph_seed,
+                                const ccb_params* params, int32_t* id_out);
+/* Admission, one iteration of every active request, retirement.  Writes the ids finished in this step (up
+ * to capacity) and their count.  Synchronous. */
+int ccb_server_step(ccb_server* server, int32_t* finished_ids, int32_t capacity, int32_t* finished_count);
+int ccb_server_status(const ccb_server* server, int32_t* queued, int32_t* active, uint64_t* bytes_in_use);
+/* done = 1 and the result (labels: n int32) once request `id` finished; the result is then released. */
+int ccb_server_result(ccb_server* server, int32_t id, int32_t* done, int32_t* labels_out, ccb_result* result);
+void ccb_server_destroy(ccb_server* server);
+
 /* ---- device recount -----------------------------------------------------------------------------
  * Objective f, cluster sizes and G = A*Z of `count` labelings of one graph, computed on the device:
  * the GPU form of the reference's post-solve recount ObjectiveBitwise (src/cc_pbils_cpu.cpp:25-53,

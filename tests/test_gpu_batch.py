@@ -69,3 +69,50 @@ def test_batch_matches_plain_and_oracle(ccb, oracle, cuda_device):
     first = [batch.result(i).objective for i in ids]
     batch.run()
     assert [batch.result(i).objective for i in ids] == first
+
+
+def _results_equal(a, b):
+    return (a.objective, a.iterations_done, a.accepted_moves, a.local_searches, a.clusters_used) == \
+        (b.objective, b.iterations_done, b.accepted_moves, b.local_searches, b.clusters_used) and \
+        np.array_equal(a.labels, b.labels)
+
+
+def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
+    """Requests served together with others, admitted at different steps under a tight memory budget and
+    a small active cap, give exactly the result of the same request served alone and of its plain solve."""
+    reqs = []
+    for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(MIX):
+        host, _ = ccb.Graph.Planted(n, max(2, k // 2), 0.5, 0.05, 0.1, 200 + i)
+        p = ccb.PbilsParams(k=k, population=pop, gww=gww, tournament=tour, iterations=iters, early_stop=early,
+                            perturbation=pert, seed=seed)
+        reqs.append((host, p))
+    alone = []
+    for host, p in reqs:
+        sv = ccb.Server()
+        i = sv.submit(host, p)
+        out = sv.drain()
+        alone.append(out[i])
+        sv.close()
+    sv = ccb.Server(hbm_budget_bytes=3 << 20, max_active=4)
+    ids = [sv.submit(host, p) for host, p in reqs]
+    # a device-generated request beside the host ones
+    gp = ccb.PbilsParams(k=6, population=16, iterations=5, early_stop=3, seed=12)
+    gid = sv.submit_generated(gp, 900, planted=True, parts=3, p_in=0.6, p_out=0.1, flip=0.05, seed=77)
+    seen_active = 0
+    out = {}
+    while True:
+        for i in sv.step():
+            out[i] = sv.result(i)
+        q, a, b = sv.status()
+        seen_active = max(seen_active, a)
+        assert a <= 4
+        if q == 0 and a == 0:
+            break
+    assert seen_active > 1
+    for j, (host, p) in enumerate(reqs):
+        want = ccb.SolveGpu(host, p)
+        assert _results_equal(alone[j], want), j
+        assert _results_equal(out[ids[j]], want), j
+    dg, _ = ccb.DeviceGraph.planted(900, 3, 0.6, 0.1, 0.05, 77)
+    assert _results_equal(out[gid], ccb.SolveGpu(dg.download(), gp))
+    sv.close()

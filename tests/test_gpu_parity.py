@@ -219,13 +219,28 @@ def test_shared_kernel_rejects_oversized_state(ccb, oracle, cuda_device):
 
 
 # 4096 < n: the streamed K <= 8 descent, state in shared memory (n * 16 B fits) and in L2 (it does not);
-# k > 8: the incremental descent, state in shared memory (n <= ~1500 at k = 12) and in L2
+# k > 8: the incremental descent with cached keys in registers (n <= 16384; counters in shared memory or L2)
+# and with everything in global memory (n > 16384)
 @pytest.mark.parametrize("n,k,density", [(4500, 2, 0.3), (5000, 8, 0.2), (9000, 3, 0.1), (13000, 6, 0.05),
                                          (20000, 5, 0.02), (1500, 12, 0.3), (3000, 40, 0.1), (6000, 20, 0.05),
-                                         (2500, 64, 0.5)])
+                                         (2500, 64, 0.5), (17000, 10, 0.01)])
 def test_streamed_descent_matches_oracle(ccb, oracle, cuda_device, n, k, density):
     bits, edges = oracle.erdos_renyi(n, density, n + k)
     p = dict(k=k, population=4, iterations=2, early_stop=10, gww=0.25, seed=5)
     want = oracle.pbils(bits, edges, make_params(**p))
     got = ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, **p))
     _same(got, want, (n, k))
+
+
+def test_solvers_sharing_a_kernel_keep_their_shared_memory(ccb, oracle, cuda_device):
+    # n = 1000 and n = 600 at k = 5 use the same descent instance (256 threads x 4 vertices, bitset in shared
+    # memory) with different shared-memory sizes; creating the smaller one last must not break the larger.
+    big_bits, big_e = oracle.erdos_renyi(1000, 0.4, 3)
+    small_bits, small_e = oracle.erdos_renyi(600, 0.4, 4)
+    p = ccb.PbilsParams(k=5, population=8, iterations=2)
+    big = ccb.Solver(ccb.DeviceGraph(_graph(ccb, big_bits, big_e)), p)
+    small = ccb.Solver(ccb.DeviceGraph(_graph(ccb, small_bits, small_e)), p)
+    assert big.describe().split(",")[1:3] == small.describe().split(",")[1:3]
+    want = oracle.pbils(big_bits, big_e, make_params(k=5, population=8, iterations=2))
+    _same(big.pbils(p), want)
+    _same(small.pbils(p), oracle.pbils(small_bits, small_e, make_params(k=5, population=8, iterations=2)))
