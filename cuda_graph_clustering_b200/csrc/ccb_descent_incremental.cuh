@@ -116,15 +116,18 @@ struct IncState {
   }
 };
 
-template <int T, bool kSmemState>
-__device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a, int slot) {
+// GainT is the population's G type (int16 narrow, int32 wide); the slot state keeps G as uint16 counters,
+// exact for every n <= 65536 (a counter is at most the degree).  Key is the move-key width: 32 bits while
+// 2 * key_bits <= 32, else 64.
+template <int T, bool kSmemState, typename GainT = int16_t, typename Key = uint32_t>
+__device__ __forceinline__ void DescentIncremental(const DescentArgs<GainT>& a, int slot) {
   constexpr int kWarps = T / kWarp;
   constexpr int U = 4;
   constexpr int KP = kMaxK;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
   __shared__ int s_stop;
-  __shared__ MoveRecord<uint32_t> s_records[2 * kWarps];
+  __shared__ MoveRecord<Key> s_records[2 * kWarps];
   __shared__ int s_off[kWarps][KP];
 
   const int tid = threadIdx.x;
@@ -158,9 +161,20 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
     const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
     for (int c = lane; c < KP; c += kWarp) off[c] = c < k ? 64 * sizes[c] + c : 0x3fffffff;
     __syncwarp();
-    const uint4* g_src = reinterpret_cast<const uint4*>(a.cur.g + static_cast<size_t>(w) * k * ld);
-    uint4* g_dst = reinterpret_cast<uint4*>(st.g);
-    for (size_t i = tid; i < static_cast<size_t>(k) * ld / 8; i += T) g_dst[i] = g_src[i];
+    if constexpr (sizeof(GainT) == 2) {
+      const uint4* g_src = reinterpret_cast<const uint4*>(a.cur.g + static_cast<size_t>(w) * k * ld);
+      uint4* g_dst = reinterpret_cast<uint4*>(st.g);
+      for (size_t i = tid; i < static_cast<size_t>(k) * ld / 8; i += T) g_dst[i] = g_src[i];
+    } else {
+      // int32 counters (all < 65536) narrowed to uint16, four per step
+      const int4* g_src = reinterpret_cast<const int4*>(a.cur.g + static_cast<size_t>(w) * k * ld);
+      uint2* g_dst = reinterpret_cast<uint2*>(st.g);
+      for (size_t i = tid; i < static_cast<size_t>(k) * ld / 4; i += T) {
+        const int4 x = g_src[i];
+        g_dst[i] = make_uint2((static_cast<uint32_t>(x.x) & 0xffffu) | (static_cast<uint32_t>(x.y) << 16),
+                              (static_cast<uint32_t>(x.z) & 0xffffu) | (static_cast<uint32_t>(x.w) << 16));
+      }
+    }
     __syncthreads();
     const uint8_t* l_src = a.cur.labels + static_cast<size_t>(w) * ld;
     for (int u = tid; u < n; u += T) {
@@ -183,10 +197,10 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
   int empty = LowestEmpty(off, k);
   const uint32_t* prev_row = nullptr;
   const uint32_t lane_bit = 1u << lane;
-  const uint32_t key_base = (1u << bits) << bits;
+  const Key key_base = (static_cast<Key>(1) << bits) << bits;
 
   while (true) {
-    uint32_t best = KeyTraits<uint32_t>::kNone;
+    Key best = KeyTraits<Key>::kNone;
     uint32_t payload = 0;
     for (int base = tid; base < n; base += U * T) {
       int own[U], kb[U], ko[U], lbd[U];
@@ -225,14 +239,14 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
         }
         const int kbest = min(kb[i], empty >= 0 ? empty : 0x7fffffff);
         const int gain = (kbest >> 6) - (ko[i] >> 6) + 1;
-        const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
+        const Key mk = static_cast<Key>(static_cast<long long>(gain) * (1ll << bits)) + key_base + static_cast<Key>(u);
         if (mk < best) {
           best = mk;
           payload = static_cast<uint32_t>(own[i]) | (static_cast<uint32_t>(kbest & 63) << 8);
         }
       }
     }
-    const MoveRecord<uint32_t> m = BlockArgMin<uint32_t, kWarps>(best, payload, s_records + parity * kWarps);
+    const MoveRecord<Key> m = BlockArgMin<Key, kWarps>(best, payload, s_records + parity * kWarps);
     if (m.key >= key_base) break;
     parity ^= 1;
 
@@ -267,6 +281,12 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<int16_t>& a
 template <int T, bool kSmemState>
 __global__ void __launch_bounds__(T, 1) k_descent_incremental(DescentArgs<int16_t> a) {
   DescentIncremental<T, kSmemState>(a, blockIdx.x);
+}
+
+// The wide form (32767 < n <= 65536, int32 population G): state in the slot's rows of `next`, 64-bit keys.
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_descent_incremental_wide(DescentArgs<int32_t> a) {
+  DescentIncremental<T, false, int32_t, unsigned long long>(a, blockIdx.x);
 }
 
 // The same descent with the cached keys owned per thread: thread t owns vertices u = t + j T, j < V

@@ -120,6 +120,11 @@ cudaError_t LaunchDescentIncremental(const SmallKPlan& p, const DescentArgs<int1
   }
 }
 
+cudaError_t LaunchDescentIncrementalWide(const DescentArgs<int32_t>& a, int grid, cudaStream_t st) {
+  k_descent_incremental_wide<1024><<<grid, 1024, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows) {
   (void)pitch;
   (void)threads;

@@ -33,6 +33,9 @@ void IncrementalRegsShape(int n, int* threads, int* vpt);
 size_t IncrementalRegsSmem(int k, int ld, int threads, int vpt, bool counters_in_smem);
 cudaError_t LaunchDescentIncremental(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                      cudaStream_t stream, bool configure);
+// Incremental descent on the wide population (int32 G, 32767 < n <= 65536, 2 <= k <= 64): 1024 threads,
+// state in global memory (IncrementalBytes per slot), no dynamic shared memory.
+cudaError_t LaunchDescentIncrementalWide(const DescentArgs<int32_t>& args, int grid, cudaStream_t stream);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);
 

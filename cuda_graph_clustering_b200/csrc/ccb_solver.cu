@@ -12,10 +12,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <deque>
 #include <map>
-#include <unordered_map>
 #include <memory>
+#include <thread>
+#include <unordered_map>
 #include <tuple>
 #include <new>
 #include <stdexcept>
@@ -189,6 +191,8 @@ size_t DescentSmem(const Plan& p, int n, int pitch, int k, int ld, int kpad) {
   return b;
 }
 
+constexpr int kMaxVerticesIncrementalWide = 65536;
+
 Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const Device& dev) {
   Plan p;
   p.wide = n > CCB_MAX_VERTICES_NARROW || ls_kernel == CCB_LS_WIDE;
@@ -251,6 +255,19 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
     p.threads = sk.threads;
     p.smem_bytes = sk.smem_bytes;
   }
+  if (p.wide && n <= kMaxVerticesIncrementalWide && k >= 2 && ls_kernel == CCB_LS_AUTO) {
+    // cached-key descent over uint16 counters: exact while every degree < 65536
+    SmallKPlan& sk = p.sk;
+    sk.k = k;
+    sk.threads = 1024;
+    sk.smem_state = false;
+    sk.smem_bytes = 0;
+    p.incremental = true;
+    p.smem_state = false;
+    p.smem_rows = false;
+    p.threads = sk.threads;
+    p.smem_bytes = 0;
+  }
   return p;
 }
 
@@ -293,6 +310,7 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 }
 
 const char* KernelName(const Plan& p) {
+  if (p.incremental && p.wide) return "incremental wide (n <= 65536, uint16 counters, 64-bit keys), L2";
   if (p.incremental) {
     if (p.sk.registers) {
       return p.smem_state ? "incremental 9 <= k <= 64, cached keys in registers, counters in shared memory"
@@ -487,7 +505,9 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   CCB_CUDA(cudaEventCreateWithFlags(&s->poll_event[1], cudaEventDisableTiming));
 
   // Shared-memory opt-in for the descent instance of this plan.
-  if (s->plan.incremental) {
+  if (s->plan.incremental && s->plan.wide) {
+    // no dynamic shared memory
+  } else if (s->plan.incremental) {
     CCB_CUDA(LaunchDescentIncremental(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
   } else if (s->plan.small_k) {
     CCB_CUDA(LaunchDescentSmallK(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
@@ -547,6 +567,13 @@ void LaunchDescentStep(ccb_solver& s, int grid, int population, int tournament, 
         e = s.plan.incremental ? LaunchDescentIncremental(s.plan.sk, a, grid, st, false)
                                : LaunchDescentSmallK(s.plan.sk, a, grid, st, false);
       });
+      CCB_CUDA(e);
+      return;
+    }
+  } else {
+    if (s.plan.incremental) {
+      cudaError_t e = cudaSuccess;
+      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentIncrementalWide(a, grid, st); });
       CCB_CUDA(e);
       return;
     }
@@ -1150,8 +1177,19 @@ struct ccb_server {
     std::chrono::steady_clock::time_point admitted;
   };
   struct Done {
+    int status = CCB_OK;
+    std::string error;
     ccb_result result{};
     std::vector<int32_t> labels;
+  };
+  // A request the batched kernels do not take (wide, k = 1, ...), solved on the plain path by a host thread
+  // of its own on a stream of its own, so its kernels overlap the batched iterations.
+  struct Side {
+    Active a;
+    cudaStream_t stream = nullptr;
+    std::thread worker;
+    std::atomic<bool> finished{false};
+    Done out;
   };
   Device device;
   size_t budget = 0;
@@ -1171,8 +1209,15 @@ struct ccb_server {
   cudaStream_t stream = nullptr;
   bool dirty = true;
   long long steps = 0;
+  std::vector<std::unique_ptr<Side>> sides;
+  int max_sides = 4;
 
   ~ccb_server() {
+    for (auto& sd : sides) {
+      if (sd->worker.joinable()) sd->worker.join();
+      if (sd->stream) cudaStreamDestroy(sd->stream);
+    }
+    sides.clear();
     active.clear();
     if (d_entries) cudaFree(d_entries);
     if (d_active) cudaFree(d_active);
@@ -1201,6 +1246,60 @@ size_t RequestBytes(const ccb_server& sv, uint32_t n, const ccb_params& p) {
          (size_t)p.population * p.k * pitch * 4 + 2 * (size_t)p.population * 4 + ld + sizeof(Control);
 }
 
+// Starts the plain solve of an admitted request on a worker thread (the request's memory stays charged to
+// the budget until it is collected).
+void StartSide(ccb_server& sv, ccb_server::Active&& a) {
+  std::unique_ptr<ccb_server::Side> sd(new ccb_server::Side());
+  sd->a = std::move(a);
+  CCB_CUDA(cudaStreamCreateWithFlags(&sd->stream, cudaStreamNonBlocking));
+  sv.in_use += sd->a.req.bytes;
+  ccb_server::Side* raw = sd.get();
+  const int device = sv.device.id;
+  raw->worker = std::thread([raw, device] {
+    ccb_server::Done& d = raw->out;
+    try {
+      CCB_CUDA(cudaSetDevice(device));
+      ccb_solver& s = *raw->a.solver;
+      d.labels.resize(s.n);
+      if (s.plan.wide) {
+        RunPbils<int32_t>(s, raw->a.req.params, raw->stream, d.labels.data(), &d.result);
+      } else {
+        RunPbils<int16_t>(s, raw->a.req.params, raw->stream, d.labels.data(), &d.result);
+      }
+    } catch (const Failure& f) {
+      d.status = f.status;
+      d.error = f.message;
+    } catch (const std::bad_alloc&) {
+      d.status = CCB_ERR_DEVICE_MEMORY;
+      d.error = "host allocation failed";
+    } catch (const std::exception& e) {
+      d.status = CCB_ERR_CUDA;
+      d.error = e.what();
+    }
+    raw->finished.store(true, std::memory_order_release);
+  });
+  sv.sides.push_back(std::move(sd));
+}
+
+// Collects the side solves that finished; appends their ids.
+void CollectSides(ccb_server& sv, std::vector<int>& finished) {
+  for (size_t i = 0; i < sv.sides.size();) {
+    ccb_server::Side& sd = *sv.sides[i];
+    if (!sd.finished.load(std::memory_order_acquire)) {
+      ++i;
+      continue;
+    }
+    sd.worker.join();
+    cudaStreamDestroy(sd.stream);
+    sd.stream = nullptr;
+    sd.out.result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - sd.a.admitted).count();
+    sv.in_use -= sd.a.req.bytes;
+    finished.push_back(sd.a.req.id);
+    sv.done[sd.a.req.id] = std::move(sd.out);
+    sv.sides.erase(sv.sides.begin() + i);
+  }
+}
+
 void Finish(ccb_server& sv, ccb_server::Active& a, const ccb_result& r, std::vector<int32_t> labels) {
   ccb_server::Done d;
   d.result = r;
@@ -1209,13 +1308,24 @@ void Finish(ccb_server& sv, ccb_server::Active& a, const ccb_result& r, std::vec
   sv.done[a.req.id] = std::move(d);
 }
 
+// Whether a request runs in the batched iterations (else on a side thread): the plan's narrow small-k or
+// incremental descents.
+bool BatchedKernelsTake(const ccb_server& sv, const ccb_server::Request& r) {
+  const int words = (int)((r.n + 31) / 32);
+  const int pitch = std::max(4, (words + 3) / 4 * 4);
+  const int ld = std::max(32, ((int)r.n + 31) / 32 * 32);
+  const Plan pl = MakePlan((int)r.n, pitch, r.params.k, ld, (r.params.k + 3) / 4 * 4, CCB_LS_AUTO, sv.device);
+  return !pl.wide && (pl.small_k || pl.incremental);
+}
+
 // Admits queued requests (FIFO) while the device-memory budget and the active-slot cap allow; a request
 // larger than the whole budget is admitted alone.  Requests the batched kernels do not take (n = 0, k = 1,
 // n > 32767) are solved on admission on the plain path.
 void Admit(ccb_server& sv) {
   while (!sv.queue.empty() && (int)sv.active.size() < sv.max_active) {
     ccb_server::Request& r = sv.queue.front();
-    if (sv.in_use + r.bytes > sv.budget && !sv.active.empty()) break;
+    if (sv.in_use + r.bytes > sv.budget && !(sv.active.empty() && sv.sides.empty())) break;
+    if ((int)sv.sides.size() >= sv.max_sides && r.n > 0 && !BatchedKernelsTake(sv, r)) break;
     ccb_server::Active a;
     a.admitted = std::chrono::steady_clock::now();
     a.req = std::move(r);
@@ -1243,14 +1353,8 @@ void Admit(ccb_server& sv) {
     a.solver.reset(MakeSolver(a.graph.get(), q.params.k, q.params.population, CCB_LS_AUTO));
     const Plan& pl = a.solver->plan;
     if (pl.wide || !(pl.small_k || pl.incremental)) {
-      std::vector<int32_t> labels(q.n);
-      ccb_result r0{};
-      if (pl.wide) {
-        RunPbils<int32_t>(*a.solver, q.params, sv.stream, labels.data(), &r0);
-      } else {
-        RunPbils<int16_t>(*a.solver, q.params, sv.stream, labels.data(), &r0);
-      }
-      Finish(sv, a, r0, std::move(labels));
+      CCB_CUDA(cudaStreamSynchronize(sv.stream));  // the graph is complete before another stream reads it
+      StartSide(sv, std::move(a));
       continue;
     }
     EnqueueInit(*a.solver, q.params, sv.stream);
@@ -1268,13 +1372,17 @@ void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t
   std::vector<int> before_ids;
   before_ids.reserve(sv.done.size());
   for (const auto& kv : sv.done) before_ids.push_back(kv.first);
+  CollectSides(sv, newly);
   Admit(sv);
-  if (sv.done.size() != done_before) {
+  if (sv.done.size() != done_before + newly.size()) {
     std::sort(before_ids.begin(), before_ids.end());
     for (const auto& kv : sv.done)
-      if (!std::binary_search(before_ids.begin(), before_ids.end(), kv.first)) note(kv.first);
+      if (!std::binary_search(before_ids.begin(), before_ids.end(), kv.first) &&
+          std::find(newly.begin(), newly.end(), kv.first) == newly.end())
+        note(kv.first);
   }
   const int count = (int)sv.active.size();
+  if (count == 0 && !sv.sides.empty()) std::this_thread::sleep_for(std::chrono::microseconds(200));
   if (count > 0) {
     if (sv.dirty) {
       std::vector<BatchEntry> entries;
@@ -1559,7 +1667,7 @@ int ccb_server_status(const ccb_server* sv, int32_t* queued, int32_t* active, ui
   return Guard([&] {
     if (!sv) Fail(CCB_ERR_STATE, "null server");
     if (queued) *queued = (int32_t)sv->queue.size();
-    if (active) *active = (int32_t)sv->active.size();
+    if (active) *active = (int32_t)(sv->active.size() + sv->sides.size());
     if (bytes_in_use) *bytes_in_use = (uint64_t)sv->in_use;
   });
 }
@@ -1570,6 +1678,12 @@ int ccb_server_result(ccb_server* sv, int32_t id, int32_t* done, int32_t* labels
     auto it = sv->done.find(id);
     *done = it != sv->done.end();
     if (it == sv->done.end()) return;
+    if (it->second.status != CCB_OK) {
+      const int status = it->second.status;
+      const std::string error = it->second.error;
+      sv->done.erase(it);
+      Fail(status, error);
+    }
     if (result) *result = it->second.result;
     if (labels_out && !it->second.labels.empty()) {
       std::memcpy(labels_out, it->second.labels.data(), it->second.labels.size() * 4);

@@ -95,9 +95,11 @@ def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
         sv.close()
     sv = ccb.Server(hbm_budget_bytes=3 << 20, max_active=4)
     ids = [sv.submit(host, p) for host, p in reqs]
-    # a device-generated request beside the host ones
+    # device-generated requests beside the host ones: one batched, one beyond the narrow limit (side thread)
     gp = ccb.PbilsParams(k=6, population=16, iterations=5, early_stop=3, seed=12)
     gid = sv.submit_generated(gp, 900, planted=True, parts=3, p_in=0.6, p_out=0.1, flip=0.05, seed=77)
+    wp = ccb.PbilsParams(k=5, population=4, iterations=2, early_stop=3, seed=13)
+    wid = sv.submit_generated(wp, 34000, density=0.004, seed=78)
     seen_active = 0
     out = {}
     while True:
@@ -115,4 +117,6 @@ def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
         assert _results_equal(out[ids[j]], want), j
     dg, _ = ccb.DeviceGraph.planted(900, 3, 0.6, 0.1, 0.05, 77)
     assert _results_equal(out[gid], ccb.SolveGpu(dg.download(), gp))
+    wg = ccb.DeviceGraph.erdos_renyi(34000, 0.004, 78)
+    assert _results_equal(out[wid], ccb.SolveGpu(wg.download(), wp))
     sv.close()
