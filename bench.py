@@ -49,10 +49,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="plain")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256, help="batched workload: instances")
     ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
+    ap.add_argument("--serve-count", type=int, default=32, help="serving workload: requests")
+    ap.add_argument("--serve-rate", type=float, default=10.0, help="serving workload: Poisson arrivals per second")
+    ap.add_argument("--serve-max-n", type=int, default=50000, help="serving workload: largest n")
+    ap.add_argument("--serve-budget-gb", type=float, default=0.0, help="serving workload: HBM budget (0: 80%% free)")
     return ap.parse_args()
 
 
@@ -274,6 +278,135 @@ def run_batched(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_serving(args, rank, world, local):
+    """The serving stream (cuda_graph_clustering_b200.workloads.serving_requests, master seed 11 + rank):
+    requests arrive by a Poisson process in real time and are submitted to a ccb_server as they arrive
+    (graph generated on the device at admission); the server admits by its HBM budget and advances every
+    admitted request one iteration per step.  Latency = completion - arrival.  The baseline is a plain FIFO:
+    the same requests solved one at a time in arrival order (graph generation + ccb_solver_pbils + label
+    copy, timed per request), its completion times computed from those service times and the arrivals.
+    Every served result is checked equal to its plain result."""
+    import torch
+
+    import cuda_graph_clustering_b200 as ccb
+    from cuda_graph_clustering_b200.workloads import serving_requests
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
+    reqs = serving_requests(args.serve_count, args.serve_rate, master=11 + rank, max_n=args.serve_max_n,
+                            population=64, iterations=50)
+
+    def params(r):
+        return ccb.PbilsParams(k=r.k, population=r.population, iterations=r.iterations,
+                               early_stop=r.iterations, seed=r.seed)
+
+    def submit(sv, r):
+        if r.erdos_renyi:
+            return sv.submit_generated(params(r), r.n, density=r.density, seed=r.graph_seed)
+        return sv.submit_generated(params(r), r.n, planted=True, parts=r.parts, p_in=r.p_in, p_out=r.p_out,
+                                   flip=r.flip, seed=r.graph_seed)
+
+    def plain(r):
+        if r.erdos_renyi:
+            g = ccb.DeviceGraph.erdos_renyi(r.n, r.density, r.graph_seed)
+        else:
+            g = ccb.DeviceGraph.planted(r.n, r.parts, r.p_in, r.p_out, r.flip, r.graph_seed)[0]
+        s_ = ccb.Solver(g, params(r))
+        out = s_.pbils(params(r))
+        s_.close()
+        g.close()
+        return out
+
+    # warm-up: module loading and first-launch costs of every kernel family on a few small requests
+    warm = [r for _, r in serving_requests(64, 1.0, master=1000 + rank, max_n=3000)][:max(args.warmup, 3)]
+    sv = ccb.Server(hbm_budget_bytes=int(args.serve_budget_gb * 2**30))
+    for r in warm:
+        submit(sv, r)
+        plain(r)
+    sv.drain()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    clocks.start()
+    finish = {}
+    results = {}
+    ids = {}
+    nxt = 0
+    peak_active = 0
+    t0 = time.perf_counter()
+    while len(finish) < len(reqs):
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and reqs[nxt][0] <= now:
+            ids[submit(sv, reqs[nxt][1])] = nxt
+            nxt += 1
+        q, a, _ = sv.status()
+        peak_active = max(peak_active, a)
+        if q == 0 and a == 0:
+            if nxt < len(reqs):
+                time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
+            continue
+        for i in sv.step():
+            finish[ids[i]] = time.perf_counter() - t0
+            results[ids[i]] = sv.result(i)
+    t_serve = max(finish.values())
+    clock_info = clocks.stop()
+    sv.close()
+
+    service = []
+    exact = True
+    for j, (_, r) in enumerate(reqs):
+        t1 = time.perf_counter()
+        w = plain(r)
+        service.append(time.perf_counter() - t1)
+        g = results[j]
+        exact &= (w.objective == g.objective and w.iterations_done == g.iterations_done
+                  and w.accepted_moves == g.accepted_moves and bool((w.labels == g.labels).all()))
+    fifo = []
+    free_at = 0.0
+    for (arr, _), sdur in zip(reqs, service):
+        free_at = max(free_at, arr) + sdur
+        fifo.append(free_at)
+    t_fifo = fifo[-1]
+    vals = torch.tensor([t_serve, t_fifo], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ts_all, tf_all = vals[0].item(), vals[1].item()
+    if rank == 0:
+        lat_s = [finish[j] - reqs[j][0] for j in range(len(reqs))]
+        lat_f = [fifo[j] - reqs[j][0] for j in range(len(reqs))]
+        count = len(reqs)
+        line = {
+            "metric": "serving solves/s", "value": world * count / ts_all, "unit": "solves/s", "n_gpus": world,
+            "steps": 1, "warmup": len(warm), "ms_per_step": 1e3 * ts_all, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16/int32", "data": "synthetic",
+            "config": {"workload": f"serving: {count} requests (first of the seeded stream, master seed 11 + rank), "
+                                   f"Poisson {args.serve_rate}/s, ER or planted, n log-uniform [500, "
+                                   f"{args.serve_max_n}], density [0.01, 0.5], k 2..32, pop 64, 50 iterations; "
+                                   "graphs generated on the device at admission",
+                       "parallelism": f"replicas x{world}",
+                       "hbm_budget_bytes": int(args.serve_budget_gb * 2**30) or "80% of free"},
+            "plain_fifo_solves_per_s": world * count / tf_all,
+            "speedup_vs_plain_fifo": tf_all / ts_all,
+            "latency_s": {"served_p50": percentile(sorted(lat_s), 0.5), "served_p99": percentile(sorted(lat_s), 0.99),
+                          "plain_fifo_p50": percentile(sorted(lat_f), 0.5),
+                          "plain_fifo_p99": percentile(sorted(lat_f), 0.99)},
+            "peak_active": peak_active,
+            "bit_exact_vs_plain": bool(exact),
+            "clocks": clock_info,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -282,6 +415,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args, rank, world, local)
+        return
+    if args.workload == "serving":
+        run_serving(args, rank, world, local)
         return
 
     import numpy as np

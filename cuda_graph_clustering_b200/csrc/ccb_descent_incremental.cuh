@@ -40,8 +40,27 @@ __device__ __forceinline__ int2 RescanBest2(const uint16_t* g, int ld, int u, co
   return make_int2(b1, b2);
 }
 
-__device__ __forceinline__ int RescanBest(const uint16_t* g, int ld, int u, const int* off, int k, int own) {
-  return RescanBest2(g, ld, u, off, k, own).x;
+// Smallest and second smallest key over the non-empty clusters c != own of vertex u, computed by the whole
+// warp for one vertex: lane l reads clusters l and l + 32, then two warp reductions.  Every lane gets the
+// result.  Keys are distinct (the cluster index is in the low bits), so exactly one lane holds the minimum.
+__device__ __forceinline__ int2 WarpRescan2(const uint16_t* g, int ld, int u, const int* off, int k, int own) {
+  const int lane = threadIdx.x % kWarp;
+  int k1 = 0x7fffffff, k2 = 0x7fffffff;
+  if (lane < k) {
+    const int o = off[lane];
+    if (lane != own && o >= 64) k1 = o - 128 * static_cast<int>(g[static_cast<size_t>(lane) * ld + u]);
+  }
+  if (lane + kWarp < k) {
+    const int o = off[lane + kWarp];
+    if (lane + kWarp != own && o >= 64) {
+      k2 = o - 128 * static_cast<int>(g[static_cast<size_t>(lane + kWarp) * ld + u]);
+    }
+  }
+  const int lo = min(k1, k2);
+  const int hi = max(k1, k2);
+  const int b1 = __reduce_min_sync(kAllLanes, lo);
+  const int b2 = __reduce_min_sync(kAllLanes, lo == b1 ? hi : lo);
+  return make_int2(b1, b2);
 }
 
 // Lowest-index empty cluster from a warp's off[] row, or -1.  An empty cluster c has size 0 and no
@@ -54,24 +73,18 @@ __device__ __forceinline__ int LowestEmpty(const int* off, int k) {
   return lo ? __ffs(lo) - 1 : (hi ? 32 + __ffs(hi) - 1 : -1);
 }
 
-// Folds the move (from -> to, `moved` = the vertex that moved) into the cached keys of vertex u, whose
-// counters G_from, G_to are already updated to gf, gt.  kb is the smallest key over the non-empty foreign
+// Folds the move (from -> to, `moved` = the vertex that moved) into the cached keys of vertex u, given its
+// new keys kf = key_from(u) and kt = key_to(u).  kb is the smallest key over the non-empty foreign
 // clusters, lb a lower bound on the second smallest, ko the key of u's own cluster (label = ko & 63).
 // Only key_from and key_to changed; every other foreign cluster but kb's is still >= lb.  So the best
-// known key is exact whenever it stays below lb, and all k lanes are rescanned only when it does not (the
-// cached best got worse than the bound) or for the moved vertex, whose foreign set changed.  After the move
-// `to` is non-empty; if `from` became empty it leaves the set.
-__device__ __forceinline__ void FoldMove(int u, int gf, int gt, int from, int to, int moved, bool from_empty,
-                                         const uint16_t* g, int ld, const int* off, int k, int& kb, int& lb,
-                                         int& ko) {
-  const int kf = off[from] - 128 * gf;
-  const int kt = off[to] - 128 * gt;
+// known key is exact whenever it stays below lb.  Returns true when it does not (the cached best got worse
+// than the bound) or for the moved vertex, whose foreign set changed: then kb and lb must be rescanned.
+// After the move `to` is non-empty; if `from` became empty it leaves the set.
+__device__ __forceinline__ bool FoldMove(int u, int kf, int kt, int from, int to, int moved, bool from_empty,
+                                         int& kb, int& lb, int& ko) {
   if (u == moved) {
     ko = kt;
-    const int2 r = RescanBest2(g, ld, u, off, k, to);
-    kb = r.x;
-    lb = r.y;
-    return;
+    return true;
   }
   const int own = ko & 63;
   if (own == from) ko = kf;
@@ -90,12 +103,11 @@ __device__ __forceinline__ void FoldMove(int u, int gf, int gt, int from, int to
   if (m1 < lb) {
     kb = m1;
     lb = min(lb, m2);
-  } else {
-    const int2 r = RescanBest2(g, ld, u, off, k, own);
-    kb = r.x;
-    lb = r.y;
+    return false;
   }
+  return true;
 }
+
 // Shared or global layout of one slot's incremental state (all arrays indexed by vertex, leading dimension ld).
 struct IncState {
   uint16_t* g;    // [k][ld] counters G_c(u), cluster-major: the two lanes a move touches are contiguous
@@ -202,47 +214,73 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<GainT>& a, 
   while (true) {
     Key best = KeyTraits<Key>::kNone;
     uint32_t payload = 0;
-    for (int base = tid; base < n; base += U * T) {
-      int own[U], kb[U], ko[U], lbd[U];
+    const bool fold = prev_row != nullptr;
+    const int offf = fold ? off[from] : 0;
+    const int offt = fold ? off[to] : 0;
+    // warp-uniform trip count: the rescans below are warp-cooperative
+    for (int base0 = tid - lane; base0 < n; base0 += U * T) {
+      const int base = base0 + lane;
+      int kb[U], ko[U], lbd[U], gf[U], gt[U];
       uint32_t rw[U];
 #pragma unroll
       for (int i = 0; i < U; ++i) {
         const int u = base + i * T;
-        if (u < n) {
-          own[i] = st.lab[u];
-          kb[i] = st.kbest[u];
-          ko[i] = st.kown[u];
-          lbd[i] = st.kbound[u];
-          rw[i] = prev_row != nullptr ? prev_row[u >> 5] : 0u;
+        const bool live = u < n;
+        kb[i] = live ? st.kbest[u] : 0x7fffffff;
+        ko[i] = live ? st.kown[u] : 0;
+        lbd[i] = live ? st.kbound[u] : 0x7fffffff;
+        rw[i] = live && fold ? prev_row[u >> 5] : 0u;
+        gf[i] = live && fold ? st.g[static_cast<size_t>(from) * ld + u] : 0;
+        gt[i] = live && fold ? st.g[static_cast<size_t>(to) * ld + u] : 0;
+      }
+      unsigned need = 0, chg = 0;  // bit i: rescan needed / cached keys changed
+      if (fold) {
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+          const int u = base + i * T;
+          if (u >= n) continue;
+          if (rw[i] & lane_bit) {
+            st.g[static_cast<size_t>(from) * ld + u] = static_cast<uint16_t>(--gf[i]);
+            st.g[static_cast<size_t>(to) * ld + u] = static_cast<uint16_t>(++gt[i]);
+          }
+          const int kb0 = kb[i], ko0 = ko[i], lb0 = lbd[i];
+          if (FoldMove(u, offf - 128 * gf[i], offt - 128 * gt[i], from, to, moved, from_empty, kb[i], lbd[i],
+                       ko[i])) {
+            need |= 1u << i;
+          }
+          chg |= static_cast<unsigned>(kb[i] != kb0 || ko[i] != ko0 || lbd[i] != lb0) << i;
+          if (u == moved) st.lab[u] = static_cast<uint8_t>(to);
+        }
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+          unsigned m = __ballot_sync(kAllLanes, (need >> i) & 1u);
+          while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int own_l = __shfl_sync(kAllLanes, ko[i] & 63, l);
+            const int2 r = WarpRescan2(st.g, ld, base0 + l + i * T, off, k, own_l);
+            if (lane == l) {
+              kb[i] = r.x;
+              lbd[i] = r.y;
+            }
+          }
         }
       }
 #pragma unroll
       for (int i = 0; i < U; ++i) {
         const int u = base + i * T;
         if (u >= n) continue;
-        if (prev_row != nullptr) {
-          uint16_t* g_from = st.g + static_cast<size_t>(from) * ld + u;
-          uint16_t* g_to = st.g + static_cast<size_t>(to) * ld + u;
-          int gf = *g_from;
-          int gt = *g_to;
-          if (rw[i] & lane_bit) {
-            *g_from = static_cast<uint16_t>(--gf);
-            *g_to = static_cast<uint16_t>(++gt);
-          }
-          const int kb0 = kb[i], ko0 = ko[i], lb0 = lbd[i];
-          FoldMove(u, gf, gt, from, to, moved, from_empty, st.g, ld, off, k, kb[i], lbd[i], ko[i]);
-          if (u == moved) st.lab[u] = static_cast<uint8_t>(to);
-          own[i] = ko[i] & 63;
-          if (kb[i] != kb0) st.kbest[u] = kb[i];
-          if (ko[i] != ko0) st.kown[u] = ko[i];
-          if (lbd[i] != lb0) st.kbound[u] = lbd[i];
+        if ((chg | need) >> i & 1u) {
+          st.kbest[u] = kb[i];
+          st.kown[u] = ko[i];
+          st.kbound[u] = lbd[i];
         }
         const int kbest = min(kb[i], empty >= 0 ? empty : 0x7fffffff);
         const int gain = (kbest >> 6) - (ko[i] >> 6) + 1;
         const Key mk = static_cast<Key>(static_cast<long long>(gain) * (1ll << bits)) + key_base + static_cast<Key>(u);
         if (mk < best) {
           best = mk;
-          payload = static_cast<uint32_t>(own[i]) | (static_cast<uint32_t>(kbest & 63) << 8);
+          payload = static_cast<uint32_t>(ko[i] & 63) | (static_cast<uint32_t>(kbest & 63) << 8);
         }
       }
     }
@@ -387,6 +425,8 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
   while (true) {
     uint32_t best = KeyTraits<uint32_t>::kNone;
     uint32_t payload = 0;
+    const int offf = pending ? off[from] : 0;
+    const int offt = pending ? off[to] : 0;
     // with the keys in shared memory nothing is indexed by j in registers: one group body, looped
 #pragma unroll(kSmemKeys ? 1 : V / kGroup)
     for (int j0 = 0; j0 < V; j0 += kGroup) {
@@ -409,25 +449,59 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
           cko[i] = sko[(j0 + i) * T + tid];
         }
       }
+      unsigned need = 0, chg = 0;  // bit i: rescan needed / cached keys changed
+      if (pending) {
 #pragma unroll
-      for (int i = 0; i < kGroup; ++i) {
-        const int j = j0 + i;
-        if (!((valid >> j) & 1)) continue;
-        const int u = tid + j * T;
-        int& kbj = kSmemKeys ? ckb[i] : kb[kSmemKeys ? 0 : j];
-        int& lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
-        int& koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
-        if (pending) {
+        for (int i = 0; i < kGroup; ++i) {
+          const int j = j0 + i;
+          if (!((valid >> j) & 1)) continue;
+          const int u = tid + j * T;
+          int& kbj = kSmemKeys ? ckb[i] : kb[kSmemKeys ? 0 : j];
+          int& lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
+          int& koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
           if (rw[i] & lane_bit) {
             g[static_cast<size_t>(from) * ld + u] = static_cast<uint16_t>(--gf[i]);
             g[static_cast<size_t>(to) * ld + u] = static_cast<uint16_t>(++gt[i]);
           }
           const int kb0 = kbj, lb0 = lbj, ko0 = koj;
-          FoldMove(u, gf[i], gt[i], from, to, moved, from_empty, g, ld, off, k, kbj, lbj, koj);
-          if constexpr (kSmemKeys) {
-            if (kbj != kb0) skb[j * T + tid] = kbj;
-            if (lbj != lb0) slb[j * T + tid] = lbj;
-            if (koj != ko0) sko[j * T + tid] = koj;
+          if (FoldMove(u, offf - 128 * gf[i], offt - 128 * gt[i], from, to, moved, from_empty, kbj, lbj, koj)) {
+            need |= 1u << i;
+          }
+          chg |= static_cast<unsigned>(kbj != kb0 || lbj != lb0 || koj != ko0) << i;
+        }
+        // warp-cooperative rescans, one vertex at a time
+#pragma unroll
+        for (int i = 0; i < kGroup; ++i) {
+          const int j = j0 + i;
+          int& kbj = kSmemKeys ? ckb[i] : kb[kSmemKeys ? 0 : j];
+          int& lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
+          const int koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
+          unsigned m = __ballot_sync(kAllLanes, (need >> i) & 1u);
+          while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int own_l = __shfl_sync(kAllLanes, koj & 63, l);
+            const int2 r = WarpRescan2(g, ld, tid - lane + l + j * T, off, k, own_l);
+            if (lane == l) {
+              kbj = r.x;
+              lbj = r.y;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kGroup; ++i) {
+        const int j = j0 + i;
+        if (!((valid >> j) & 1)) continue;
+        const int u = tid + j * T;
+        const int kbj = kSmemKeys ? ckb[i] : kb[kSmemKeys ? 0 : j];
+        const int lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
+        const int koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
+        if constexpr (kSmemKeys) {
+          if ((chg | need) >> i & 1u) {
+            skb[j * T + tid] = kbj;
+            slb[j * T + tid] = lbj;
+            sko[j * T + tid] = koj;
           }
         }
         const int kbest = min(kbj, empty >= 0 ? empty : 0x7fffffff);
