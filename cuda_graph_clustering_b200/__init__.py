@@ -10,16 +10,19 @@ sm_100a kernels; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import _native
-from ._native import (CcbError, CcbParams, CcbResult, CcbKernelStats, LS_AUTO, LS_GLOBAL, LS_SHARED, LS_WIDE,
+from ._native import (CcbError, CcbParams, CcbResult, CcbKernelStats, CcbTuningEntry, LS_AUTO, LS_GLOBAL, LS_SHARED, LS_WIDE,
                       MAX_CLUSTERS, MAX_VERTICES_NARROW, MAX_VERTICES_WIDE, check, lib)
 
 __all__ = ["Graph", "PbilsParams", "PbilsResult", "SolveGpu", "SolveNeighborhoodGpu",
-           "SolveNeighborhoodWithManyLocalSearchesGpu", "DeviceGraph", "Solver", "Batch", "CcbError", "LS_AUTO", "LS_GLOBAL",
+           "SolveNeighborhoodWithManyLocalSearchesGpu", "DeviceGraph", "Solver", "Batch", "Server", "CcbError",
+           "set_tuning", "get_tuning", "load_tuning", "LS_AUTO", "LS_GLOBAL",
            "LS_SHARED", "LS_WIDE", "MAX_CLUSTERS", "kMaxClusters"]
 
 kMaxClusters = MAX_CLUSTERS  # include/cc_gpu.hpp:10
@@ -278,12 +281,52 @@ def evaluate_labelings_noalloc(bits_ptr: int, n: int, words_per_row: int, edges:
                                                sizes_ptr, g_ptr, stream or None))
 
 
+TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+TUNING_FIELDS = ("kind", "n_min", "n_max", "k_min", "k_max", "use_kind", "threads", "blocks_per_sm", "max_slots")
+_tuning_loaded = False
+
+
+def set_tuning(entries: list) -> None:
+    """Installs a batched-engine tuning table (ccb_tuning_set): a list of dicts with TUNING_FIELDS."""
+    arr = (CcbTuningEntry * max(len(entries), 1))()
+    for i, e in enumerate(entries):
+        arr[i] = CcbTuningEntry(*[int(e[f]) for f in TUNING_FIELDS])
+    check(lib().ccb_tuning_set(arr, len(entries)))
+
+
+def get_tuning() -> list:
+    count = C.c_int32()
+    check(lib().ccb_tuning_get(None, 0, C.byref(count)))
+    arr = (CcbTuningEntry * max(count.value, 1))()
+    check(lib().ccb_tuning_get(arr, count.value, C.byref(count)))
+    return [{f: getattr(arr[i], f) for f in TUNING_FIELDS} for i in range(count.value)]
+
+
+def load_tuning(path: str | None = None) -> bool:
+    """Installs the committed table written by cuda_graph_clustering_b200.autotune (tuning.json beside this
+    module) if present; returns whether one was installed.  Batch and Server call it once on first use."""
+    global _tuning_loaded
+    _tuning_loaded = True
+    path = path or TUNING_PATH
+    if not os.path.exists(path):
+        return False
+    with open(path) as f:
+        set_tuning(json.load(f)["entries"])
+    return True
+
+
+def _ensure_tuning() -> None:
+    if not _tuning_loaded:
+        load_tuning()
+
+
 class Batch:
     """Many independent PBILS instances solved together (ccb_batch_*): one CUDA graph per iteration of all
     instances, persistent per-bucket descent kernels fed by a device work queue.  Each result equals the
     instance's plain solve bit for bit."""
 
     def __init__(self):
+        _ensure_tuning()
         h = C.c_void_p()
         check(lib().ccb_batch_create(C.byref(h)))
         self.handle = h
@@ -329,6 +372,7 @@ class Server:
     other admitted request, and retire when they finish.  Each result equals the request's plain solve."""
 
     def __init__(self, hbm_budget_bytes: int = 0, max_active: int = 0):
+        _ensure_tuning()
         h = C.c_void_p()
         check(lib().ccb_server_create(hbm_budget_bytes, max_active, C.byref(h)))
         self.handle = h

@@ -42,6 +42,12 @@ class CcbKernelStats(C.Structure):
                 ("record_launches", C.c_int64), ("other_launches", C.c_int64)]
 
 
+class CcbTuningEntry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_min", C.c_int32), ("n_max", C.c_int32), ("k_min", C.c_int32),
+                ("k_max", C.c_int32), ("use_kind", C.c_int32), ("threads", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("max_slots", C.c_int32)]
+
+
 _u32p = C.POINTER(C.c_uint32)
 _i32p = C.POINTER(C.c_int32)
 _vp = C.c_void_p
@@ -75,6 +81,8 @@ SIGNATURES = {
     "ccb_batch_result": (C.c_int, [_vp, C.c_int32, _vp, C.POINTER(CcbResult)]),
     "ccb_batch_describe": (C.c_char_p, [_vp]),
     "ccb_batch_destroy": (None, [_vp]),
+    "ccb_tuning_set": (C.c_int, [C.POINTER(CcbTuningEntry), C.c_int32]),
+    "ccb_tuning_get": (C.c_int, [C.POINTER(CcbTuningEntry), C.c_int32, C.POINTER(C.c_int32)]),
     "ccb_server_create": (C.c_int, [C.c_uint64, C.c_int32, C.POINTER(_vp)]),
     "ccb_server_submit": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(CcbParams),
                                     C.POINTER(C.c_int32)]),

@@ -40,6 +40,8 @@ struct BatchShape {
   int vpt = 4;          // register form
   bool smem = false;    // register form: bitset in shared memory; streamed / incremental: state in shared memory
   size_t smem_bytes = 0;
+  int blocks_per_sm = 0;  // tuned resident slots per SM (0: the occupancy limit)
+  int max_slots = 0;      // tuned cap on slots running at once (0: none)
   int grid = 0;
 };
 

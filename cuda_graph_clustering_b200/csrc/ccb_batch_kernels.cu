@@ -59,8 +59,10 @@ __global__ void __launch_bounds__(T, 1) kb_descent_stream(const BatchEntry* __re
   }
 }
 
+// 1024 / T resident blocks per SM fit the register file (the body needs no more than 64 registers).
 template <int T, bool S>
-__global__ void __launch_bounds__(T, 1) kb_descent_incremental(const BatchEntry* __restrict__ entries, BatchQueue q) {
+__global__ void __launch_bounds__(T, 1024 / T) kb_descent_incremental(const BatchEntry* __restrict__ entries,
+                                                                      BatchQueue q) {
   __shared__ int s_item;
   int entry, slot;
   while (ClaimItem(q, &s_item, entry, slot)) {

@@ -16,6 +16,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <unordered_map>
 #include <tuple>
@@ -881,7 +882,36 @@ BatchEntry MakeEntry(const ccb_solver& s, const ccb_params& p) {
   return e;
 }
 
+std::mutex g_tuning_mutex;
+std::vector<ccb_tuning_entry> g_tuning;
+
+// The plan's batched kernel, then the first matching tuning entry applied to it.
+BatchShape ShapeOfPlan(const ccb_solver& s);
+
 BatchShape ShapeOf(const ccb_solver& s) {
+  BatchShape sh = ShapeOfPlan(s);
+  std::lock_guard<std::mutex> lock(g_tuning_mutex);
+  for (const ccb_tuning_entry& t : g_tuning) {
+    if ((t.kind >= 0 && t.kind != sh.kind) || s.n < t.n_min || s.n > t.n_max || s.k < t.k_min || s.k > t.k_max) {
+      continue;
+    }
+    if (t.use_kind == kBatchIncremental && !s.plan.smem_state &&
+        (sh.kind == kBatchIncrementalRegs || sh.kind == kBatchIncremental) &&
+        (t.threads == 256 || t.threads == 512 || t.threads == 1024)) {
+      sh.kind = kBatchIncremental;  // the slot's rows of `next` hold IncrementalBytes: the global-state form fits
+      sh.threads = t.threads;
+      sh.vpt = 4;
+      sh.smem = false;
+      sh.smem_bytes = 0;
+    }
+    sh.blocks_per_sm = std::max(0, t.blocks_per_sm);
+    sh.max_slots = std::max(0, t.max_slots);
+    break;
+  }
+  return sh;
+}
+
+BatchShape ShapeOfPlan(const ccb_solver& s) {
   BatchShape sh;
   const SmallKPlan& sk = s.plan.sk;
   sh.k = s.k;
@@ -919,10 +949,10 @@ void BuildWorkLists(WorkLists& w, const std::vector<const ccb_solver*>& solvers,
                     double l2_share) {
   w.ReleaseBuckets();
   const int count = (int)solvers.size();
-  std::map<std::tuple<int, int, int, int, int>, int> index;
+  std::map<std::tuple<int, int, int, int, int, int, int>, int> index;
   for (int e = 0; e < count; ++e) {
     const BatchShape sh = ShapeOf(*solvers[e]);
-    const auto key = std::make_tuple(sh.kind, sh.k, sh.threads, sh.vpt, (int)sh.smem);
+    const auto key = std::make_tuple(sh.kind, sh.k, sh.threads, sh.vpt, (int)sh.smem, sh.blocks_per_sm, sh.max_slots);
     auto it = index.find(key);
     if (it == index.end()) {
       it = index.emplace(key, (int)w.buckets.size()).first;
@@ -978,16 +1008,18 @@ void BuildWorkLists(WorkLists& w, const std::vector<const ccb_solver*>& solvers,
     WorkLists::Bucket& bk = w.buckets[i];
     size_t state = 0;
     for (int m : bk.members) state = std::max(state, L2StateBytes(*solvers[m]));
-    const int per_sm = BatchDescentBlocksPerSm(bk.shape);
+    int per_sm = BatchDescentBlocksPerSm(bk.shape);
+    if (bk.shape.blocks_per_sm > 0) per_sm = std::min(per_sm, bk.shape.blocks_per_sm);
     long long grid = (long long)per_sm * dev.sms;
     if (state > 0 && l2_share > 0.0) {
       grid = std::min<long long>(grid, std::max<long long>(1, (long long)(l2_share * dev.l2_bytes / state)));
     }
+    if (bk.shape.max_slots > 0) grid = std::min<long long>(grid, bk.shape.max_slots);
     bk.shape.grid = (int)std::max<long long>(1, std::min<long long>(grid, bk.total));
     CCB_CUDA(LaunchBatchDescent(bk.shape, nullptr, BatchQueue{}, nullptr, true));
     CCB_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
     CCB_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
-    char line[160];
+    char line[200];
     std::snprintf(line, sizeof(line), "%s k=%d threads=%d vpt=%d smem=%d: %zu instances, %d slots, grid %d; ",
                   bk.shape.kind == kBatchRegisters          ? "registers"
                   : bk.shape.kind == kBatchStream           ? "stream"
@@ -1607,6 +1639,22 @@ int ccb_batch_result(const ccb_batch* b, int32_t id, int32_t* labels_out, ccb_re
 const char* ccb_batch_describe(const ccb_batch* b) { return b ? b->work.description.c_str() : ""; }
 
 void ccb_batch_destroy(ccb_batch* b) { delete b; }
+
+int ccb_tuning_set(const ccb_tuning_entry* entries, int32_t count) {
+  return Guard([&] {
+    if (count < 0 || (count > 0 && !entries)) Fail(CCB_ERR_INVALID, "bad tuning table");
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    g_tuning.assign(entries, entries + count);
+  });
+}
+
+int ccb_tuning_get(ccb_tuning_entry* entries, int32_t capacity, int32_t* count) {
+  return Guard([&] {
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    if (count) *count = (int32_t)g_tuning.size();
+    for (int32_t i = 0; entries && i < capacity && i < (int32_t)g_tuning.size(); ++i) entries[i] = g_tuning[i];
+  });
+}
 
 int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server** out) {
   return Guard([&] {

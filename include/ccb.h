@@ -159,6 +159,28 @@ int ccb_batch_result(const ccb_batch* batch, int32_t id, int32_t* labels_out, cc
 const char* ccb_batch_describe(const ccb_batch* batch);
 void ccb_batch_destroy(ccb_batch* batch);
 
+/* ---- batched-engine tuning ------------------------------------------------------------------------
+ * No counterpart in the reference.  A process-wide table, written by the project's autotuner
+ * (cuda_graph_clustering_b200/autotune.py, table committed as tuning.json), that picks per shape bucket of
+ * the batched engine the descent kernel, its threads per slot and its resident block count.  Batches and
+ * servers built after ccb_tuning_set use it; an instance matches the first entry whose kind and n, k
+ * ranges contain it.  Tuning never changes a result: every choice runs the same trajectory. */
+typedef struct ccb_tuning_entry {
+  int32_t kind;          /* the plan's batched kernel: 0 registers, 1 streamed, 2 incremental with its state in
+                            global memory, 3 incremental with cached keys in registers / shared memory; -1 any */
+  int32_t n_min, n_max;  /* inclusive */
+  int32_t k_min, k_max;
+  int32_t use_kind;      /* -1: the plan's kernel; 2: the incremental kernel with its state in global memory
+                            (taken by kind-2 and kind-3 instances whose state is not in shared memory) */
+  int32_t threads;       /* threads per slot for use_kind 2: 256, 512 or 1024 */
+  int32_t blocks_per_sm; /* resident slots per SM of the persistent grid; 0: the occupancy limit */
+  int32_t max_slots;     /* cap on the slots running at once (the L2-resident block count); 0: none */
+} ccb_tuning_entry;
+/* Replaces the table (count 0 clears it). */
+int ccb_tuning_set(const ccb_tuning_entry* entries, int32_t count);
+/* Copies up to capacity entries; count receives the table size. */
+int ccb_tuning_get(ccb_tuning_entry* entries, int32_t capacity, int32_t* count);
+
 /* ---- serving ------------------------------------------------------------------------------------
  * No counterpart in the reference.  A request loop with continuous batching: submitted requests wait in a
  * FIFO queue; every ccb_server_step admits queued requests while their estimated device memory (graph rows

@@ -93,3 +93,33 @@ def test_empty_graph_pbils_needs_no_device(ccb):
     assert (r.objective, r.iterations_done, r.local_searches, r.clusters_used) == (0, 7, 21, 0)
     r = ccb.SolveGpu(ccb.Graph(0), ccb.PbilsParams(iterations=7, early_stop=0))
     assert r.iterations_done == 1
+
+
+def test_tuning_table_roundtrip(ccb):
+    entries = [dict(kind=3, n_min=8193, n_max=16384, k_min=9, k_max=64, use_kind=2, threads=256, blocks_per_sm=0,
+                    max_slots=0),
+               dict(kind=1, n_min=4097, n_max=32767, k_min=2, k_max=8, use_kind=-1, threads=0, blocks_per_sm=1,
+                    max_slots=148)]
+    before = ccb.get_tuning()
+    try:
+        ccb.set_tuning(entries)
+        assert ccb.get_tuning() == entries
+        ccb.set_tuning([])
+        assert ccb.get_tuning() == []
+        with pytest.raises(ccb.CcbError):
+            ccb.check(ccb.lib().ccb_tuning_set(None, 1))
+    finally:
+        ccb.set_tuning(before)
+
+
+def test_committed_tuning_table_is_well_formed(ccb):
+    path = ccb.TUNING_PATH
+    if not os.path.exists(path):
+        pytest.skip("no tuning table committed")
+    import json
+    table = json.load(open(path))
+    for e in table["entries"]:
+        assert set(e) == set(ccb.TUNING_FIELDS)
+        assert e["kind"] in (-1, 0, 1, 2, 3) and e["use_kind"] in (-1, 2)
+        assert e["n_min"] <= e["n_max"] and e["k_min"] <= e["k_max"]
+        assert e["use_kind"] == -1 or e["threads"] in (256, 512, 1024)

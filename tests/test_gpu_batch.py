@@ -71,6 +71,38 @@ def test_batch_matches_plain_and_oracle(ccb, oracle, cuda_device):
     assert [batch.result(i).objective for i in ids] == first
 
 
+@pytest.mark.parametrize("table", [
+    [dict(kind=-1, n_min=0, n_max=1 << 20, k_min=0, k_max=64, use_kind=2, threads=256, blocks_per_sm=0,
+          max_slots=0)],
+    [dict(kind=-1, n_min=0, n_max=1 << 20, k_min=0, k_max=64, use_kind=2, threads=512, blocks_per_sm=1,
+          max_slots=3)],
+    [dict(kind=-1, n_min=0, n_max=1 << 20, k_min=0, k_max=64, use_kind=-1, threads=0, blocks_per_sm=2,
+          max_slots=0)],
+])
+def test_tuned_batch_matches_plain(ccb, cuda_device, table):
+    """Every tuning choice (global-state kernel, threads per slot, resident blocks, slot cap) runs the same
+    trajectories."""
+    before = ccb.get_tuning()
+    ccb.set_tuning(table)
+    try:
+        batch = ccb.Batch()
+        runs = []
+        extra = [(9000, 20, 8, 0.1, 5, 2, 6, 0.4, 11), (17000, 12, 6, 0.1, 5, 2, 6, 0.4, 12),
+                 (6000, 40, 10, 0.1, 5, 2, 6, 0.4, 13)]
+        for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(MIX + extra):
+            dg, _ = ccb.DeviceGraph.planted(n, max(2, k // 2), 0.5, 0.05, 0.1, 300 + i)
+            p = ccb.PbilsParams(k=k, population=pop, gww=gww, tournament=tour, iterations=iters,
+                                early_stop=early, perturbation=pert, seed=seed)
+            runs.append((dg, p, batch.add(dg, p)))
+        batch.run()
+        for dg, p, i in runs:
+            got = batch.result(i)
+            want = ccb.SolveGpu(dg.download(), p)
+            assert _results_equal(got, want), (i, batch.describe())
+    finally:
+        ccb.set_tuning(before)
+
+
 def _results_equal(a, b):
     return (a.objective, a.iterations_done, a.accepted_moves, a.local_searches, a.clusters_used) == \
         (b.objective, b.iterations_done, b.accepted_moves, b.local_searches, b.clusters_used) and \
