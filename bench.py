@@ -213,13 +213,20 @@ def run_batched(args, rank, world, local):
                               gww=0.1, seed=i.seed) for i in mix]
     batch = ccb.Batch()
     ids = [batch.add(g, p) for g, p in zip(graphs, params)]
+    # warm-up: one iteration of a batch of every instance shape (module loading, first launches, graph
+    # instantiation paths), not the timed batch itself, whose run takes minutes
+    warm = ccb.Batch()
+    for g, i in zip(graphs, mix):
+        warm.add(g, ccb.PbilsParams(k=i.k, population=i.population, iterations=1, early_stop=1, gww=0.1,
+                                    seed=i.seed + 1))
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
     for _ in range(args.warmup):
-        batch.run()
+        warm.run()
+    warm.close()
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()

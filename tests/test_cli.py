@@ -1,0 +1,62 @@
+"""The cc_gpu command line mirror: edge-list loading and argument handling on the CPU; a full run on the GPU
+checked against the oracle, with the reference's result-JSON keys and labels file."""
+import json
+
+import pytest
+
+from oracle import make_params
+
+
+def test_edge_list_ranks_ids_and_skips_comments(tmp_path):
+    from cuda_graph_clustering_b200.cli import load_edge_list
+
+    p = tmp_path / "e.txt"
+    p.write_text("# comment\n% other\nsrc,dst\n10 20\n20 30 extra\n30,10\n5 5\n100\t10\n")
+    g = load_edge_list(str(p))
+    # ids 5, 10, 20, 30, 100 -> vertices 0..4; the self-loop on 5 keeps its vertex but adds no edge
+    assert g.n == 5 and g.edges == 4
+    pairs = {(1, 2), (2, 3), (3, 1), (4, 1)}
+    for i in range(5):
+        for j in range(5):
+            assert g.IsJoined(i, j) == ((i, j) in pairs or (j, i) in pairs)
+
+
+def test_edge_list_without_edges_is_an_error(tmp_path, capsys):
+    from cuda_graph_clustering_b200.cli import main
+
+    p = tmp_path / "empty.txt"
+    p.write_text("# nothing\n")
+    assert main(["--edges", str(p)]) == 1
+    assert "error: no edges in" in capsys.readouterr().out
+
+
+def test_parser_defaults_match_reference_params():
+    from cuda_graph_clustering_b200.cli import parser
+
+    a = parser().parse_args([])
+    assert (a.k, a.pop, a.tournament, a.iters, a.early_stop, a.perturb, a.gww, a.seed) == \
+        (2, 128, 5, 100, 6, 0.4, 0.1, 1)
+    assert a.algorithm == "pbils" and a.ls_kernel == "auto" and a.verify
+
+
+@pytest.mark.gpu
+def test_cli_run_writes_reference_json(tmp_path, oracle, cuda_device, capsys):
+    from cuda_graph_clustering_b200.cli import main
+
+    out, labels = tmp_path / "r.json", tmp_path / "l.txt"
+    rc = main(["--n", "300", "--density", "0.3", "--graph-seed", "4", "--k", "4", "--pop", "16", "--iters", "6",
+               "--runs", "2", "--out", str(out), "--labels-out", str(labels)])
+    assert rc == 0
+    text = capsys.readouterr().out
+    assert "verified" in text and "objective    min=" in text
+    r = json.loads(out.read_text())
+    keys = ["algorithm", "backend", "size", "edges", "density", "k", "population", "gww", "runs",
+            "objective function value", "objective average", "objective max", "computation time seconds",
+            "computation time average", "clusters used", "clustering vector"]
+    assert list(r) == keys
+    bits, edges = oracle.erdos_renyi(300, 0.3, 4)
+    runs = [oracle.pbils(bits, edges, make_params(k=4, population=16, iterations=6, seed=s)) for s in (1, 2)]
+    best = min(runs, key=lambda x: x.objective)
+    assert r["objective function value"] == best.objective and r["objective max"] == max(x.objective for x in runs)
+    assert r["clustering vector"] == [int(x) for x in best.labels]
+    assert [int(x) for x in labels.read_text().split()] == [int(x) for x in best.labels]
