@@ -40,7 +40,13 @@ PLAIN_OBJECTIVE = {1: 234911}  # seed -> objective of the CPU oracle (and the re
 # pop 128; a step is a short solve (3 iterations) because one iteration costs ~10^4 moves per slot.
 NORTH = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournament=5, perturbation=0.4, gww=0.1,
              iterations=3, early_stop=100, seed=1)
-WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "north": (NORTH, {})}
+# The wide configuration: G(65536, 0.02) (a 512 MiB bitset) from graph seed 1, k = 2 or 3 on the packed wide
+# descents (int32 G), pop 128, gww 0.1, 50 iterations.  No CPU objective is known at this size: every step's
+# labels are recounted on the GPU instead (ccb_evaluate_labelings) and must give the reported objective.
+WIDE2 = dict(n=65536, density=0.02, graph_seed=1, k=2, population=128, tournament=5, perturbation=0.4, gww=0.1,
+             iterations=50, early_stop=50, seed=1)
+WIDE3 = dict(WIDE2, k=3)
+WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "north": (NORTH, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {})}
 
 
 def parse():
@@ -443,7 +449,10 @@ def main():
     cfg, objectives = WORKLOADS[args.workload]
     cfg = dict(cfg)
     seed = cfg["seed"] + rank
-    graph = ccb.Graph.ErdosRenyi(cfg["n"], cfg["density"], cfg["graph_seed"])
+    if cfg["n"] > 20000:  # the device generator gives the same bits in milliseconds
+        graph = ccb.DeviceGraph.erdos_renyi(cfg["n"], cfg["density"], cfg["graph_seed"]).download()
+    else:
+        graph = ccb.Graph.ErdosRenyi(cfg["n"], cfg["density"], cfg["graph_seed"])
     params = ccb.PbilsParams(k=cfg["k"], population=cfg["population"], tournament=cfg["tournament"],
                              perturbation=cfg["perturbation"], gww=cfg["gww"], iterations=cfg["iterations"],
                              early_stop=cfg["early_stop"], seed=seed)
@@ -501,10 +510,21 @@ def main():
     barrier()
     t0 = time.perf_counter()
     e2e_ok = True
+    e2e_results = []
     for _ in range(args.steps):
         r = ccb.SolveGpu(g_pinned, params)
+        e2e_results.append(r)
         e2e_ok &= (expected is None or r.objective == expected)
     e2e_s = time.perf_counter() - t0
+    recount_ok = None
+    if expected is None:
+        # size-independent check: the labels returned recount on the GPU to the reported objective, and the
+        # e2e solves (same seed) give the device-resident solves' objective
+        from cuda_graph_clustering_b200.cli import recount
+
+        recount_ok = all(recount(graph, np.asarray(r.labels), cfg["k"]) == r.objective for r in e2e_results[:1])
+        recount_ok &= all(r.objective == results[0].objective for r in e2e_results)
+        bit_exact = recount_ok and all(r.objective == results[0].objective for r in results)
 
     # ---- max over ranks ------------------------------------------------------------------------
     vals = torch.tensor([total_ms, e2e_s, float(iters), float(moves)], dtype=torch.float64, device="cuda")
@@ -528,12 +548,21 @@ def main():
         # (k*ld*2 + ld) and the labels written out (ld)
         per_move = n * (k * 2 + 1) + 4 * words + 8 * deg
         per_launch = moves_per_launch * per_move + pop * (k * ld * 2 + 2 * ld)
+        if cfg["n"] > 32767 and k in (2, 3):
+            # packed wide descent: per move the slot's words (4 or 8 bytes per vertex), the moved vertex's row
+            # and the changed words of its neighbours; per slot the int32 G and labels read, labels written
+            wb = 4 if k == 2 else 8
+            per_move = wb * n + 4 * words + wb * deg
+            per_launch = moves_per_launch * per_move + pop * (k * ld * 4 + 2 * ld + wb * n)
         peak, peak_kind = measured_peak_hbm()
         achieved = per_launch / (descent_ms * 1e-3) / 1e9
         traffic = profiled_traffic(f"k_descent_{args.workload}")
         value = iters_all / (total_ms_all * 1e-3)
         cpu = None
-        if not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
+        if cfg["n"] > 32767:
+            cpu = {"value": None, "unit": "iter/s", "cores": None, "kind": "reference",
+                   "sample": "not run: one CPU iteration at this size takes minutes (17-52 G popcounts per rebuild)"}
+        elif not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
             sample = 20 if args.workload == "plain" else 1
             t, f, threads = reference_cpu_run(cfg, sample)
             cpu = {"value": sample / t, "unit": "iter/s", "cores": threads, "kind": "reference",
@@ -542,7 +571,8 @@ def main():
         line = {
             "metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32" if n > 32767 else "int16",
+            "data": "synthetic",
             "config": {"workload": f"{args.workload} PBILS: ER(n={n}, p={cfg['density']}, graph seed "
                                    f"{cfg['graph_seed']}), k={k}, pop={pop}, tournament 5, perturb 0.4, gww 0.1, "
                                    f"{cfg['iterations']} iterations (early stop off), seed {cfg['seed']} + rank",
@@ -550,6 +580,7 @@ def main():
                        "kernel_plan": solver.describe()},
             "ls_moves_per_s": moves_all / (total_ms_all * 1e-3),
             "bit_exact": bit_exact,
+            "recount_ok": recount_ok,
             "objective": results[0].objective,
             "e2e": {"value": iters_all / e2e_all, "unit": "iter/s",
                     "h2d_bytes_per_step": int(graph.bits.nbytes), "d2h_bytes_per_step": int(4 * n + 48),

@@ -1,0 +1,212 @@
+// Steepest descent on the wide path (32767 < n <= 2^20) for k = 2 and k = 3 with the slot's state packed into
+// one word per vertex, so the whole population's state stays resident in L2 (k = 2: 4 bytes per vertex,
+// 32 MiB for n = 65536 and 128 slots; k = 3: 8 bytes, 64 MiB).  Same trajectory as k_descent and the
+// reference's BestMove/ApplyMove (src/cc_pbils_cpu.cpp:99-139); the reference's own packed wide kernels are
+// KernelLocalSearch2Wide / KernelLocalSearch3Wide (cuda/cc_local_search_k2.cuh:132-221,
+// cuda/cc_local_search_k3.cuh:28-127).
+//
+// k = 2: word = 2 e + a with e = G_1(u) - G_0(u) and a the label.  With s = size_1 - size_0 the only move of
+//        u has gain d = s + 1 - 2e (a = 0) or 2 - d (a = 1).  A move of v to cluster t adds +-2 to e of every
+//        neighbour (word +-4) and flips a(v).
+// k = 3: word = G_0 | G_1 << 20 | G_2 << 40 | a << 60.  Per vertex h_c = size_c - 2 G_c, the best foreign
+//        target is the smallest 4 h_c + c over c != a and its gain is h_c - h_a + 1.  A move of v from f to t
+//        adds 2^(20 t) - 2^(20 f) to every neighbour's word (no borrow: G_f >= 1 there) and rewrites a(v).
+// Each thread owns the vertices u = j T + tid; the update of the previous move is folded into the next scan
+// (one pass over the state per move), and a word is stored back only when it changed.
+#pragma once
+
+#include <cstdint>
+
+#include "ccb_device.cuh"
+#include "ccb_streams.cuh"
+
+namespace ccb {
+
+template <int K>
+struct WidePacked;
+
+template <>
+struct WidePacked<2> {
+  using Word = int32_t;
+  static constexpr int kGroup = 16;  // vertices whose loads are in flight together
+  struct Sizes {
+    int s;  // size_1 - size_0
+  };
+  __device__ static Word Make(const int32_t* g, int ld, int u, int a) {
+    return 2 * (g[ld + u] - g[u]) + a;
+  }
+  __device__ static int Label(Word w) { return w & 1; }
+  __device__ static void LoadSizes(const int32_t* sizes, Sizes& z) { z.s = sizes[1] - sizes[0]; }
+  __device__ static void Apply(Sizes& z, int from, int to) { z.s += to == 1 ? 2 : -2; }
+  // neighbour of the moved vertex / the moved vertex itself
+  __device__ static Word Neighbour(Word w, int from, int to) { return w + (to == 1 ? 4 : -4); }
+  __device__ static Word Moved(Word w, int to) { return (w & ~1) | to; }
+  // gain of the vertex's best move and its target
+  __device__ static int Gain(Word w, const Sizes& z, int& target) {
+    const int a = w & 1;
+    const int d = z.s + 1 - (w >> 1) * 2;
+    target = a ^ 1;
+    return a ? 2 - d : d;
+  }
+};
+
+template <>
+struct WidePacked<3> {
+  using Word = unsigned long long;
+  static constexpr int kGroup = 8;
+  struct Sizes {
+    int n0, n1, n2;
+  };
+  __device__ static Word Make(const int32_t* g, int ld, int u, int a) {
+    return static_cast<Word>(g[u]) | static_cast<Word>(g[ld + u]) << 20 | static_cast<Word>(g[2 * ld + u]) << 40 |
+           static_cast<Word>(a) << 60;
+  }
+  __device__ static int Label(Word w) { return static_cast<int>(w >> 60); }
+  __device__ static void LoadSizes(const int32_t* sizes, Sizes& z) {
+    z.n0 = sizes[0];
+    z.n1 = sizes[1];
+    z.n2 = sizes[2];
+  }
+  __device__ static void Apply(Sizes& z, int from, int to) {
+    z.n0 += (to == 0) - (from == 0);
+    z.n1 += (to == 1) - (from == 1);
+    z.n2 += (to == 2) - (from == 2);
+  }
+  __device__ static Word Neighbour(Word w, int from, int to) {
+    return w + (static_cast<Word>(1) << (20 * to)) - (static_cast<Word>(1) << (20 * from));
+  }
+  __device__ static Word Moved(Word w, int to) {
+    return (w & ((static_cast<Word>(1) << 60) - 1)) | static_cast<Word>(to) << 60;
+  }
+  __device__ static int Gain(Word w, const Sizes& z, int& target) {
+    constexpr Word kMask = (1u << 20) - 1;
+    const int a = static_cast<int>(w >> 60);
+    const int h0 = z.n0 - 2 * static_cast<int>(w & kMask);
+    const int h1 = z.n1 - 2 * static_cast<int>((w >> 20) & kMask);
+    const int h2 = z.n2 - 2 * static_cast<int>((w >> 40) & kMask);
+    const int k0 = a == 0 ? 0x7fffffff : 4 * h0;
+    const int k1 = a == 1 ? 0x7fffffff : 4 * h1 + 1;
+    const int k2 = a == 2 ? 0x7fffffff : 4 * h2 + 2;
+    const int best = min(k0, min(k1, k2));
+    const int ha = a == 0 ? h0 : (a == 1 ? h1 : h2);
+    target = best & 3;
+    return (best >> 2) - ha + 1;
+  }
+};
+
+template <int K, int T>
+__device__ __forceinline__ void DescentWidePacked(const DescentArgs<int32_t>& a, int slot) {
+  using P = WidePacked<K>;
+  using Word = typename P::Word;
+  using Key = unsigned long long;
+  constexpr int kWarps = T / kWarp;
+  constexpr int U = P::kGroup;
+  __shared__ int s_winner;
+  __shared__ int s_stop;
+  __shared__ MoveRecord<Key> s_records[2 * kWarps];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int n = a.gr.n;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+  const int pitch = a.gr.pitch;
+
+  if (tid == 0) {
+    s_stop = a.ctl->stop;
+    if (!s_stop) {
+      const int64_t* f = a.cur.f;
+      s_winner = a.tournament > 0 ? TournamentWinner(a.select_stream, slot, a.iteration, a.population, a.tournament,
+                                                     [f](int i) { return f[i]; })
+                                  : slot;
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const int w = s_winner;
+
+  // the slot's words in its rows of `next` (k * ld int32 per slot: room for ld words of 4 or 8 bytes)
+  Word* state = reinterpret_cast<Word*>(a.next.g + static_cast<size_t>(slot) * a.k * ld);
+  {
+    const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
+    const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
+    for (int u = tid; u < n; u += T) state[u] = P::Make(g, ld, u, lab[u]);
+  }
+  typename P::Sizes z;
+  P::LoadSizes(a.cur.sizes + static_cast<size_t>(w) * a.kpad, z);
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+
+  unsigned long long applied = 0;
+  int parity = 0;
+  int from = 0, to = 0, moved = -1;
+  bool pending = false;
+  const uint32_t* prev_row = a.gr.bits;
+  const uint32_t lane_bit = 1u << lane;
+  const Key key_base = (static_cast<Key>(1) << bits) << bits;
+
+  while (true) {
+    Key best = KeyTraits<Key>::kNone;
+    uint32_t payload = 0;
+    for (int j0 = 0; j0 * T < n; j0 += U) {  // block-uniform trip count
+      Word wd[U];
+      uint32_t rw[U];
+#pragma unroll
+      for (int i = 0; i < U; ++i) {
+        const int u = (j0 + i) * T + tid;
+        const bool live = u < n;
+        wd[i] = live ? state[u] : Word{};
+        rw[i] = live && pending ? prev_row[u >> 5] : 0u;
+      }
+#pragma unroll
+      for (int i = 0; i < U; ++i) {
+        const int u = (j0 + i) * T + tid;
+        if (u >= n) continue;
+        if (pending) {
+          const Word old = wd[i];
+          if (rw[i] & lane_bit) wd[i] = P::Neighbour(wd[i], from, to);
+          if (u == moved) wd[i] = P::Moved(wd[i], to);
+          if (wd[i] != old) state[u] = wd[i];
+        }
+        int target;
+        const int gain = P::Gain(wd[i], z, target);
+        if (gain < 0) {
+          const Key mk = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(u);
+          if (mk < best) {
+            best = mk;
+            payload = static_cast<uint32_t>(P::Label(wd[i])) | static_cast<uint32_t>(target) << 8;
+          }
+        }
+      }
+    }
+    const MoveRecord<Key> m = BlockArgMin<Key, kWarps>(best, payload, s_records + parity * kWarps);
+    if (m.key >= key_base) break;
+    parity ^= 1;
+    moved = MoveVertex(m.key, bits);
+    from = static_cast<int>(m.payload & 0xff);
+    to = static_cast<int>(m.payload >> 8);
+    P::Apply(z, from, to);
+    prev_row = a.gr.bits + static_cast<size_t>(moved) * pitch;
+    pending = true;
+    objective += MoveDelta(m.key, bits);
+    ++applied;
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      break;
+    }
+  }
+
+  uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
+  for (int u = tid; u < n; u += T) dst[u] = static_cast<uint8_t>(P::Label(state[u]));
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
+template <int K, int T>
+__global__ void __launch_bounds__(T, 1) k_descent_wide_packed(DescentArgs<int32_t> a) {
+  DescentWidePacked<K, T>(a, blockIdx.x);
+}
+
+}  // namespace ccb

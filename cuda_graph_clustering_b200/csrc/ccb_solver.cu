@@ -153,6 +153,7 @@ struct Plan {
   int key_bits = 0;
   bool small_k = false;     // the packed K <= 8 descents (registers / streamed)
   bool incremental = false; // the incremental 9 <= k <= 64 descent
+  bool packed_wide = false;  // the packed wide descent (k = 2, 3)
   SmallKPlan sk;
 };
 
@@ -256,6 +257,16 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
     p.threads = sk.threads;
     p.smem_bytes = sk.smem_bytes;
   }
+  if (p.wide && (k == 2 || k == 3) && ls_kernel == CCB_LS_AUTO) {
+    // one packed word per vertex: the population's state stays in L2
+    p.packed_wide = true;
+    p.sk.k = k;
+    p.threads = 1024;
+    p.smem_state = false;
+    p.smem_rows = false;
+    p.smem_bytes = 0;
+    return p;
+  }
   if (p.wide && n <= kMaxVerticesIncrementalWide && k >= 2 && ls_kernel == CCB_LS_AUTO) {
     // cached-key descent over uint16 counters: exact while every degree < 65536
     SmallKPlan& sk = p.sk;
@@ -311,6 +322,10 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 }
 
 const char* KernelName(const Plan& p) {
+  if (p.packed_wide) {
+    return p.sk.k == 3 ? "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2"
+                       : "packed wide k = 2 (e = G1 - G0 and the label, 4 bytes per vertex), L2";
+  }
   if (p.incremental && p.wide) return "incremental wide (n <= 65536, uint16 counters, 64-bit keys), L2";
   if (p.incremental) {
     if (p.sk.registers) {
@@ -506,7 +521,7 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   CCB_CUDA(cudaEventCreateWithFlags(&s->poll_event[1], cudaEventDisableTiming));
 
   // Shared-memory opt-in for the descent instance of this plan.
-  if (s->plan.incremental && s->plan.wide) {
+  if ((s->plan.incremental && s->plan.wide) || s->plan.packed_wide) {
     // no dynamic shared memory
   } else if (s->plan.incremental) {
     CCB_CUDA(LaunchDescentIncremental(s->plan.sk, DescentArgs<int16_t>{}, 0, nullptr, true));
@@ -572,6 +587,12 @@ void LaunchDescentStep(ccb_solver& s, int grid, int population, int tournament, 
       return;
     }
   } else {
+    if (s.plan.packed_wide) {
+      cudaError_t e = cudaSuccess;
+      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentWidePacked(a, grid, st); });
+      CCB_CUDA(e);
+      return;
+    }
     if (s.plan.incremental) {
       cudaError_t e = cudaSuccess;
       s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentIncrementalWide(a, grid, st); });

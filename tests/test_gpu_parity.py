@@ -199,10 +199,12 @@ def test_wide_path_beyond_narrow_limit(ccb, oracle, cuda_device, k):
     assert oracle.objective_bitwise(bits, got.labels) == got.objective
 
 
-@pytest.mark.parametrize("n,k,density", [(40000, 12, 0.02), (50000, 30, 0.01), (65536, 3, 0.005)])
-def test_wide_incremental_matches_generic_wide(ccb, oracle, cuda_device, n, k, density):
-    """Beyond the narrow limit the auto plan runs the cached-key descent on uint16 counters with 64-bit move
-    keys (up to n = 65536); the forced generic wide kernel (int32 G, full scan) must give the same run."""
+@pytest.mark.parametrize("n,k,density", [(40000, 12, 0.02), (50000, 30, 0.01), (65536, 2, 0.005),
+                                         (65536, 3, 0.005), (70000, 2, 0.002), (70000, 3, 0.002)])
+def test_wide_auto_matches_generic_wide(ccb, oracle, cuda_device, n, k, density):
+    """Beyond the narrow limit the auto plan runs the packed descents for k = 2, 3 (one word per vertex) and
+    the cached-key descent on uint16 counters with 64-bit move keys for larger k (up to n = 65536); the
+    forced generic wide kernel (int32 G, full scan) must give the same run."""
     g = ccb.DeviceGraph.erdos_renyi(n, density, 5 + k).download()
     p = dict(k=k, population=4, iterations=2, early_stop=10, seed=k)
     auto = ccb.SolveGpu(g, _params(ccb, **p))
