@@ -550,9 +550,13 @@ def main():
         per_launch = moves_per_launch * per_move + pop * (k * ld * 2 + 2 * ld)
         if cfg["n"] > 32767 and k in (2, 3):
             # packed wide descent: per move the slot's words (4 or 8 bytes per vertex), the moved vertex's row
-            # and the changed words of its neighbours; per slot the int32 G and labels read, labels written
+            # and the changed words of its neighbours; per slot the int32 G and labels read, labels written.
+            # The degree-proportional forms read no full scan per move: the moved vertex's row and a read and
+            # a write of each neighbour's word (their rescans, rare, are not counted).
             wb = 4 if k == 2 else 8
             per_move = wb * n + 4 * words + wb * deg
+            if "degree-proportional" in solver.describe():
+                per_move = 4 * words + 2 * wb * deg
             per_launch = moves_per_launch * per_move + pop * (k * ld * 4 + 2 * ld + wb * n)
         peak, peak_kind = measured_peak_hbm()
         achieved = per_launch / (descent_ms * 1e-3) / 1e9

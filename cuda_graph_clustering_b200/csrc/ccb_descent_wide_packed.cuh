@@ -209,4 +209,238 @@ __global__ void __launch_bounds__(T, 1) k_descent_wide_packed(DescentArgs<int32_
   DescentWidePacked<K, T>(a, blockIdx.x);
 }
 
+// k = 2 with work per move proportional to the moved vertex's degree instead of n.  With s = size_1 - size_0
+// the gain of a vertex is s + 1 - 2e in cluster 0 and 1 - s + 2e in cluster 1, so within a cluster the best
+// move is the largest e (cluster 0) or the smallest e (cluster 1), ties to the lower vertex, whatever s is.
+// Every thread keeps, for the vertices it owns, the best vertex of each cluster; the block minimum over the
+// threads' two candidates is the move (smallest gain, then lowest vertex).  A move of v to cluster t changes
+// e by the same +-2 for every neighbour: in one cluster all neighbours get better (a compare against the
+// thread's best), in the other they get worse (the thread rescans its vertices only if its best was among
+// them), and v changes cluster.  A thread owns the row words {32 W j + 32 i + lane : i < W} of its warp's
+// stretch (W words per thread), so the row of v is read coalesced and a rescan reads 128-byte runs.
+struct WideBest2 {
+  int e0, u0;  // cluster 0: largest e, lowest vertex (u0 < 0: none)
+  int e1, u1;  // cluster 1: smallest e, lowest vertex
+  __device__ void Clear() {
+    e0 = e1 = 0;
+    u0 = u1 = -1;
+  }
+  __device__ void Offer(int w, int u) {
+    const int e = w >> 1;
+    if (w & 1) {
+      if (u1 < 0 || e < e1 || (e == e1 && u < u1)) e1 = e, u1 = u;
+    } else {
+      if (u0 < 0 || e > e0 || (e == e0 && u < u0)) e0 = e, u0 = u;
+    }
+  }
+};
+
+// Recomputes lane `owner`'s two bests with the whole warp: the owner's vertices are the 32 of each of its row
+// words, lane l reads vertex l of every word (128-byte runs), and two warp reductions pick the best of each
+// cluster.  Keys: cluster 0 max of (e + 2^20) << 11 | (2047 - j), cluster 1 min of (e + 2^20) << 11 | j, with
+// j = 32 i + lane the vertex's place among the owner's (lower j = lower vertex); e > -2^20 keeps both
+// sentinels (0 and ~0) out of reach.
+template <int W>
+__device__ __forceinline__ void WarpRescanWide2(const int32_t* state, int n, int words, int owner_word0, int owner,
+                                                WideBest2& b) {
+  const int lane = threadIdx.x % kWarp;
+  uint32_t k0 = 0u, k1 = ~0u;
+#pragma unroll(W < 8 ? W : 8)
+  for (int i = 0; i < W; ++i) {
+    const int q = owner_word0 + i * kWarp;
+    const int u = 32 * q + lane;
+    if (q < words && u < n) {
+      const int wd = state[u];
+      const uint32_t j = static_cast<uint32_t>(i * kWarp + lane);
+      const uint32_t e = static_cast<uint32_t>((wd >> 1) + (1 << 20));
+      if (wd & 1) {
+        k1 = min(k1, e << 11 | j);
+      } else {
+        k0 = max(k0, e << 11 | (2047u - j));
+      }
+    }
+  }
+  k0 = __reduce_max_sync(kAllLanes, k0);
+  k1 = __reduce_min_sync(kAllLanes, k1);
+  if (lane == owner) {
+    b.Clear();
+    if (k0 != 0u) {
+      const int j = 2047 - static_cast<int>(k0 & 2047u);
+      b.e0 = static_cast<int>(k0 >> 11) - (1 << 20);
+      b.u0 = 32 * (owner_word0 + (j / kWarp) * kWarp) + j % kWarp;
+    }
+    if (k1 != ~0u) {
+      const int j = static_cast<int>(k1 & 2047u);
+      b.e1 = static_cast<int>(k1 >> 11) - (1 << 20);
+      b.u1 = 32 * (owner_word0 + (j / kWarp) * kWarp) + j % kWarp;
+    }
+  }
+}
+
+template <int T, int W>
+__device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a, int slot) {
+  using Key = unsigned long long;
+  constexpr int kWarps = T / kWarp;
+  __shared__ int s_winner;
+  __shared__ int s_stop;
+  __shared__ MoveRecord<Key> s_records[2 * kWarps];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = a.gr.n;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+  const int pitch = a.gr.pitch;
+  const int words = (n + 31) / 32;
+  const int word0 = warp * kWarp * W + lane;  // this thread's row words: word0 + 32 i, i < W
+
+  if (tid == 0) {
+    s_stop = a.ctl->stop;
+    if (!s_stop) {
+      const int64_t* f = a.cur.f;
+      s_winner = a.tournament > 0 ? TournamentWinner(a.select_stream, slot, a.iteration, a.population, a.tournament,
+                                                     [f](int i) { return f[i]; })
+                                  : slot;
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const int w = s_winner;
+
+  int32_t* state = a.next.g + static_cast<size_t>(slot) * a.k * ld;
+  WideBest2 b;
+  b.Clear();
+  {
+    const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
+    const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
+    // the warp builds its owners' words 32 at a time (vertex 32 q + lane of each of its words q)
+    const int warp_word0 = warp * kWarp * W;
+#pragma unroll 1
+    for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+      const int u = 32 * q + lane;
+      if (u < n) state[u] = 2 * (g[ld + u] - g[u]) + lab[u];
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int owner = 0; owner < kWarp; ++owner) WarpRescanWide2<W>(state, n, words, warp_word0 + owner, owner, b);
+  }
+  const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+  int s = sizes[1] - sizes[0];
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+  unsigned long long applied = 0;
+  int parity = 0;
+  const Key key_base = (static_cast<Key>(1) << bits) << bits;
+
+  while (true) {
+    Key best = KeyTraits<Key>::kNone;
+    uint32_t payload = 0;
+    if (b.u0 >= 0) {
+      const int gain = s + 1 - 2 * b.e0;
+      if (gain < 0) {
+        best = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(b.u0);
+        payload = 0u | 1u << 8;
+      }
+    }
+    if (b.u1 >= 0) {
+      const int gain = 1 - s + 2 * b.e1;
+      if (gain < 0) {
+        const Key mk = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(b.u1);
+        if (mk < best) {
+          best = mk;
+          payload = 1u;
+        }
+      }
+    }
+    const MoveRecord<Key> m = BlockArgMin<Key, kWarps>(best, payload, s_records + parity * kWarps);
+    if (m.key >= key_base) break;
+    parity ^= 1;
+    const int v = MoveVertex(m.key, bits);
+    const int to = static_cast<int>(m.payload >> 8);
+    s += to == 1 ? 2 : -2;
+    objective += MoveDelta(m.key, bits);
+    ++applied;
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      break;
+    }
+    // neighbours of v: e += 2 (to = 1) or -= 2 (to = 0); the cluster whose best gets worse is 1 resp. 0
+    const int step = to == 1 ? 4 : -4;
+    const int worse = to;  // e up hurts cluster 1 (smallest e wanted), e down hurts cluster 0
+    const uint32_t* row = a.gr.bits + static_cast<size_t>(v) * pitch;
+    bool rescan = false;
+#pragma unroll(W < 4 ? W : 4)
+    for (int i = 0; i < W; ++i) {
+      const int q = word0 + i * kWarp;
+      uint32_t mbits = q < words ? row[q] : 0u;
+      const int base = 32 * (word0 + i * kWarp);
+      while (mbits) {
+        // up to four neighbours with their loads in flight together
+        int us[4];
+        int ws[4];
+        int cnt = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          us[c] = -1;
+          if (mbits) {
+            us[c] = base + __ffs(mbits) - 1;
+            mbits &= mbits - 1;
+            ++cnt;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (us[c] < 0) continue;
+          const int wd = ws[c] + step;
+          state[us[c]] = wd;
+          if ((wd & 1) == worse) {
+            rescan |= us[c] == ((wd & 1) ? b.u1 : b.u0);
+          } else {
+            b.Offer(wd, us[c]);
+          }
+        }
+        (void)cnt;
+      }
+    }
+    // v itself changes cluster (its e is unchanged: no self-loops)
+    const int qv = v >> 5;
+    if (qv >= warp * kWarp * W && qv < (warp + 1) * kWarp * W && (qv - warp * kWarp * W) % kWarp == lane) {
+      const int wd = state[v] ^ 1;
+      state[v] = wd;
+      rescan |= v == (to == 1 ? b.u0 : b.u1);
+      b.Offer(wd, v);
+    }
+    __syncwarp();  // every lane's stores are visible to the warp's rescans
+    unsigned pending = __ballot_sync(kAllLanes, rescan);
+    while (pending) {
+      const int owner = __ffs(pending) - 1;
+      pending &= pending - 1;
+      WarpRescanWide2<W>(state, n, words, warp * kWarp * W + owner, owner, b);
+    }
+  }
+
+  __syncwarp();
+  uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
+  {
+    const int warp_word0 = warp * kWarp * W;
+#pragma unroll 1
+    for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+      const int u = 32 * q + lane;
+      if (u < n) dst[u] = static_cast<uint8_t>(state[u] & 1);
+    }
+  }
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
+template <int T, int W>
+__global__ void __launch_bounds__(T, 1) k_descent_wide2_sparse(DescentArgs<int32_t> a) {
+  DescentWide2Sparse<T, W>(a, blockIdx.x);
+}
+
 }  // namespace ccb
