@@ -443,4 +443,226 @@ __global__ void __launch_bounds__(T, 1) k_descent_wide2_sparse(DescentArgs<int32
   DescentWide2Sparse<T, W>(a, blockIdx.x);
 }
 
+// k = 3 in the same degree-proportional form.  For a vertex in cluster a the gain of target c is
+// (size_c - size_a + 1) - 2 d with d = G_c - G_a, so within each of the six (a, c) classes the best vertex is
+// the largest d, ties to the lower vertex, whatever the sizes are.  Each thread keeps one key per class,
+// (d + 2^20) << 11 | (2047 - j) (j = the vertex's place among the thread's, 0: none), and its candidate is the
+// smallest (gain, vertex, target) over the six.  A move of v from f to t changes d of every neighbour in class
+// (a, c) by [c = t] - [c = f] - [a = t] + [a = f], the same for all of them: better (a compare), worse (a
+// rescan if the class's best is among them) or unchanged; v leaves the classes of f and joins those of t.
+// Vertex words as in WidePacked<3>.
+__device__ __forceinline__ int Wide3Class(int a, int c) { return 2 * a + (c > a ? c - 1 : c); }
+__device__ __forceinline__ int Wide3Target(int cls) {
+  const int a = cls >> 1, r = cls & 1;
+  return r < a ? r : r + 1;
+}
+__device__ __forceinline__ int Wide3G(unsigned long long w, int c) {
+  return static_cast<int>((w >> (20 * c)) & ((1u << 20) - 1));
+}
+
+// Folds vertex word wd (place j) into the keys of its two classes.
+__device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, uint32_t (&key)[6]) {
+  const int a = static_cast<int>(wd >> 60);
+  const int ga = Wide3G(wd, a);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (c == a) continue;
+    const uint32_t d = static_cast<uint32_t>(Wide3G(wd, c) - ga + (1 << 20));
+    const uint32_t k = d << 11 | (2047u - j);
+    const int cls = Wide3Class(a, c);
+    key[cls] = max(key[cls], k);
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void WarpRescanWide3(const unsigned long long* state, int n, int words, int owner_word0,
+                                                int owner, uint32_t (&key)[6]) {
+  const int lane = threadIdx.x % kWarp;
+  uint32_t k[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll(W < 8 ? W : 8)
+  for (int i = 0; i < W; ++i) {
+    const int q = owner_word0 + i * kWarp;
+    const int u = 32 * q + lane;
+    if (q < words && u < n) Wide3Offer(state[u], static_cast<uint32_t>(i * kWarp + lane), k);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    const uint32_t m = __reduce_max_sync(kAllLanes, k[c]);
+    if (lane == owner) key[c] = m;
+  }
+}
+
+template <int T, int W>
+__device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a, int slot) {
+  using Key = unsigned long long;
+  using Word = unsigned long long;
+  constexpr int kWarps = T / kWarp;
+  __shared__ int s_winner;
+  __shared__ int s_stop;
+  __shared__ MoveRecord<Key> s_records[2 * kWarps];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = a.gr.n;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+  const int pitch = a.gr.pitch;
+  const int words = (n + 31) / 32;
+  const int warp_word0 = warp * kWarp * W;
+  const int word0 = warp_word0 + lane;  // this thread's row words: word0 + 32 i, i < W
+
+  if (tid == 0) {
+    s_stop = a.ctl->stop;
+    if (!s_stop) {
+      const int64_t* f = a.cur.f;
+      s_winner = a.tournament > 0 ? TournamentWinner(a.select_stream, slot, a.iteration, a.population, a.tournament,
+                                                     [f](int i) { return f[i]; })
+                                  : slot;
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const int w = s_winner;
+
+  Word* state = reinterpret_cast<Word*>(a.next.g + static_cast<size_t>(slot) * a.k * ld);
+  uint32_t key[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+  {
+    const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
+    const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
+#pragma unroll 1
+    for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+      const int u = 32 * q + lane;
+      if (u < n) {
+        state[u] = static_cast<Word>(g[u]) | static_cast<Word>(g[ld + u]) << 20 |
+                   static_cast<Word>(g[2 * ld + u]) << 40 | static_cast<Word>(lab[u]) << 60;
+      }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int owner = 0; owner < kWarp; ++owner) WarpRescanWide3<W>(state, n, words, warp_word0 + owner, owner, key);
+  }
+  const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+  int sz[3] = {sizes[0], sizes[1], sizes[2]};
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+  unsigned long long applied = 0;
+  int parity = 0;
+  const Key key_base = (static_cast<Key>(1) << bits) << bits;
+
+  while (true) {
+    Key best = KeyTraits<Key>::kNone;
+    uint32_t payload = 0;
+#pragma unroll
+    for (int cls = 0; cls < 6; ++cls) {  // ascending (a, c): among equal (gain, vertex) the lower target stays
+      if (key[cls] == 0u) continue;
+      const int ca = cls >> 1, cc = Wide3Target(cls);
+      const int d = static_cast<int>(key[cls] >> 11) - (1 << 20);
+      const int gain = (sz[cc] - sz[ca] + 1) - 2 * d;
+      if (gain >= 0) continue;
+      const int j = 2047 - static_cast<int>(key[cls] & 2047u);
+      const int u = 32 * (word0 + (j / kWarp) * kWarp) + j % kWarp;
+      const Key mk = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(u);
+      if (mk < best) {
+        best = mk;
+        payload = static_cast<uint32_t>(ca) | static_cast<uint32_t>(cc) << 8;
+      }
+    }
+    const MoveRecord<Key> m = BlockArgMin<Key, kWarps>(best, payload, s_records + parity * kWarps);
+    if (m.key >= key_base) break;
+    parity ^= 1;
+    const int v = MoveVertex(m.key, bits);
+    const int from = static_cast<int>(m.payload & 0xff);
+    const int to = static_cast<int>(m.payload >> 8);
+    sz[from] -= 1;
+    sz[to] += 1;
+    objective += MoveDelta(m.key, bits);
+    ++applied;
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      break;
+    }
+    const Word step = (static_cast<Word>(1) << (20 * to)) - (static_cast<Word>(1) << (20 * from));
+    const uint32_t* row = a.gr.bits + static_cast<size_t>(v) * pitch;
+    bool rescan = false;
+#pragma unroll(W < 4 ? W : 4)
+    for (int i = 0; i < W; ++i) {
+      const int q = word0 + i * kWarp;
+      uint32_t mbits = q < words ? row[q] : 0u;
+      while (mbits) {
+        int us[4];
+        Word ws[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          us[c] = -1;
+          if (mbits) {
+            us[c] = 32 * q + __ffs(mbits) - 1;
+            mbits &= mbits - 1;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : Word{};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (us[c] < 0) continue;
+          const Word wd = ws[c] + step;
+          state[us[c]] = wd;
+          const int au = static_cast<int>(wd >> 60);
+          const uint32_t j = static_cast<uint32_t>(i * kWarp + (us[c] & 31));
+          const int ga = Wide3G(wd, au);
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            if (cc == au) continue;
+            const int delta = (cc == to) - (cc == from) - (au == to) + (au == from);
+            const int cls = Wide3Class(au, cc);
+            const uint32_t k = static_cast<uint32_t>(Wide3G(wd, cc) - ga + (1 << 20)) << 11 | (2047u - j);
+            if (delta > 0) {
+              key[cls] = max(key[cls], k);
+            } else if (delta < 0) {
+              rescan |= (key[cls] & 2047u) == (2047u - j);  // the class's best got worse
+            }
+          }
+        }
+      }
+    }
+    // v changes cluster (its counters are unchanged: no self-loops)
+    const int qv = v >> 5;
+    if (qv >= warp_word0 && qv < warp_word0 + kWarp * W && (qv - warp_word0) % kWarp == lane) {
+      const Word old = state[v];
+      const Word wd = (old & ((static_cast<Word>(1) << 60) - 1)) | static_cast<Word>(to) << 60;
+      state[v] = wd;
+      const uint32_t j = static_cast<uint32_t>(((qv - warp_word0) / kWarp) * kWarp + (v & 31));
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        if (cc != from) rescan |= (key[Wide3Class(from, cc)] & 2047u) == (2047u - j) && key[Wide3Class(from, cc)];
+      }
+      Wide3Offer(wd, j, key);
+    }
+    __syncwarp();
+    unsigned pending = __ballot_sync(kAllLanes, rescan);
+    while (pending) {
+      const int owner = __ffs(pending) - 1;
+      pending &= pending - 1;
+      WarpRescanWide3<W>(state, n, words, warp_word0 + owner, owner, key);
+    }
+  }
+
+  __syncwarp();
+  uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
+#pragma unroll 1
+  for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+    const int u = 32 * q + lane;
+    if (u < n) dst[u] = static_cast<uint8_t>(state[u] >> 60);
+  }
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
+template <int T, int W>
+__global__ void __launch_bounds__(T, 1) k_descent_wide3_sparse(DescentArgs<int32_t> a) {
+  DescentWide3Sparse<T, W>(a, blockIdx.x);
+}
+
 }  // namespace ccb

@@ -38,7 +38,8 @@ cudaError_t LaunchDescentIncremental(const SmallKPlan& plan, const DescentArgs<i
 cudaError_t LaunchDescentIncrementalWide(const DescentArgs<int32_t>& args, int grid, cudaStream_t stream);
 // Packed wide descent (k = 2 or 3, int32 population G, n > 32767): 1024 threads, one 4- or 8-byte word per
 // vertex in the slot's rows of `next`, no dynamic shared memory.
-// k = 2 with `sparse`: the degree-proportional form (per-thread best vertex of each cluster).
+// With `sparse`: the degree-proportional forms (per-thread best vertex of each cluster, k = 2, or of each
+// (cluster, target) class, k = 3).
 cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& args, int grid, bool sparse, cudaStream_t stream);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);

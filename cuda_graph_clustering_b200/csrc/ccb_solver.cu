@@ -324,7 +324,10 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 
 const char* KernelName(const Plan& p) {
   if (p.packed_wide) {
-    if (p.sk.k == 3) return "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2";
+    if (p.sk.k == 3) {
+      return p.sparse ? "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), L2"
+                      : "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2";
+    }
     return p.sparse ? "packed wide k = 2, degree-proportional (per-thread best of each cluster), L2"
                     : "packed wide k = 2 (e = G1 - G0 and the label, 4 bytes per vertex), L2";
   }
@@ -478,8 +481,8 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->ld = std::max(32, (g->n + 31) / 32 * 32);
   s->ls_kernel = ls_kernel;
   s->plan = MakePlan(g->n, g->pitch, k, s->ld, s->kpad, ls_kernel, s->device);
-  // k = 2 wide on a sparse graph (average degree <= n / 8): work per move follows the degree, not n
-  s->plan.sparse = s->plan.packed_wide && k == 2 && 2.0 * (double)g->edges <= (double)g->n * g->n / 8.0;
+  // k = 2, 3 wide on a sparse graph (average degree <= n / 8): work per move follows the degree, not n
+  s->plan.sparse = s->plan.packed_wide && 2.0 * (double)g->edges <= (double)g->n * g->n / 8.0;
 
   const size_t labels = (size_t)pop * s->ld;
   const size_t gains = labels * k;

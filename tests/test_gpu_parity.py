@@ -201,7 +201,7 @@ def test_wide_path_beyond_narrow_limit(ccb, oracle, cuda_device, k):
 
 @pytest.mark.parametrize("n,k,density", [(40000, 12, 0.02), (50000, 30, 0.01), (65536, 2, 0.005),
                                          (65536, 3, 0.005), (70000, 2, 0.002), (70000, 3, 0.002),
-                                         (34000, 2, 0.3)])
+                                         (34000, 2, 0.3), (34000, 3, 0.3), (33000, 3, 0.05)])
 def test_wide_auto_matches_generic_wide(ccb, oracle, cuda_device, n, k, density):
     """Beyond the narrow limit the auto plan runs the packed descents for k = 2, 3 (one word per vertex; for
     k = 2 on a sparse graph the degree-proportional form) and the cached-key descent on uint16 counters with
