@@ -81,6 +81,7 @@ SIGNATURES = {
     "ccb_batch_result": (C.c_int, [_vp, C.c_int32, _vp, C.POINTER(CcbResult)]),
     "ccb_batch_describe": (C.c_char_p, [_vp]),
     "ccb_batch_destroy": (None, [_vp]),
+    "ccb_release_cache": (None, []),
     "ccb_tuning_set": (C.c_int, [C.POINTER(CcbTuningEntry), C.c_int32]),
     "ccb_tuning_get": (C.c_int, [C.POINTER(CcbTuningEntry), C.c_int32, C.POINTER(C.c_int32)]),
     "ccb_server_create": (C.c_int, [C.c_uint64, C.c_int32, C.POINTER(_vp)]),

@@ -1770,6 +1770,61 @@ int ccb_server_result(ccb_server* sv, int32_t id, int32_t* done, int32_t* labels
 
 void ccb_server_destroy(ccb_server* sv) { delete sv; }
 
+namespace {
+
+// The one-call entry points keep, per host thread, the device graph and solver buffers of their last call and
+// reuse them when the next call has the same device, n, k, population and kernel choice: such a call pays
+// the bitset upload and the degree count, not the allocations (ccb_release_cache frees them).
+struct OneCallCache {
+  std::unique_ptr<ccb_solver> solver;
+  std::unique_ptr<ccb_graph> graph;
+  int device = -1;
+  uint32_t n = 0;
+  int k = 0, pop = 0, ls = 0;
+  void Release() {
+    solver.reset();
+    graph.reset();
+    device = -1;
+  }
+};
+thread_local OneCallCache t_cache;
+
+ccb_solver& CachedSolver(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges, int k, int pop,
+                         int ls_kernel) {
+  int device = 0;
+  CCB_CUDA(cudaGetDevice(&device));
+  OneCallCache& c = t_cache;
+  if (c.solver && c.device == device && c.n == n && c.k == k && c.pop == pop && c.ls == ls_kernel) {
+    const int words = (int)((n + 31) / 32);
+    if (words_per_row < (uint32_t)words) Fail(CCB_ERR_INVALID, "words_per_row < ceil(n / 32)");
+    if (bits == nullptr) Fail(CCB_ERR_INVALID, "null bitset");
+    ccb_graph& g = *c.graph;
+    g.edges = (int64_t)edges;
+    CCB_CUDA(cudaMemcpy2DAsync(g.bits, g.pitch * sizeof(uint32_t), bits, words_per_row * sizeof(uint32_t),
+                               words * sizeof(uint32_t), n, cudaMemcpyHostToDevice, nullptr));
+    FinishGraph(g, nullptr);
+    // the plan's k = 2 / 3 wide form depends on the density
+    ccb_solver& s = *c.solver;
+    s.plan.sparse = s.plan.packed_wide && 2.0 * (double)edges <= (double)n * n / 8.0;
+    return s;
+  }
+  c.Release();
+  std::unique_ptr<ccb_graph> g(MakeGraph(bits, false, n, words_per_row, edges, nullptr));
+  std::unique_ptr<ccb_solver> s(MakeSolver(g.get(), k, pop, ls_kernel));
+  c.graph = std::move(g);
+  c.solver = std::move(s);
+  c.device = device;
+  c.n = n;
+  c.k = k;
+  c.pop = pop;
+  c.ls = ls_kernel;
+  return *c.solver;
+}
+
+}  // namespace
+
+void ccb_release_cache(void) { t_cache.Release(); }
+
 int ccb_pbils_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                     const ccb_params* params, int32_t* labels_out, ccb_result* result) {
   return Guard([&] {
@@ -1782,12 +1837,11 @@ int ccb_pbils_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_row, ui
       EmptyPbils(*params, result);
       return;
     }
-    std::unique_ptr<ccb_graph> g(MakeGraph(bits, false, n, words_per_row, edges, nullptr));
-    std::unique_ptr<ccb_solver> s(MakeSolver(g.get(), params->k, params->population, params->ls_kernel));
-    if (s->plan.wide) {
-      RunPbils<int32_t>(*s, *params, nullptr, labels_out, result);
+    ccb_solver& s = CachedSolver(bits, n, words_per_row, edges, params->k, params->population, params->ls_kernel);
+    if (s.plan.wide) {
+      RunPbils<int32_t>(s, *params, nullptr, labels_out, result);
     } else {
-      RunPbils<int16_t>(*s, *params, nullptr, labels_out, result);
+      RunPbils<int16_t>(s, *params, nullptr, labels_out, result);
     }
     result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
   });
@@ -1801,13 +1855,12 @@ int ccb_neighborhood_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_
     const auto started = std::chrono::steady_clock::now();
     CheckNeighborhood(*params, n);
     std::memset(result, 0, sizeof(*result));
-    std::unique_ptr<ccb_graph> g(MakeGraph(bits, false, n, words_per_row, edges, nullptr));
     const int batch = std::min<int>(params->population, (int)n);
-    std::unique_ptr<ccb_solver> s(MakeSolver(g.get(), 2, batch, params->ls_kernel));
-    if (s->plan.wide) {
-      RunNeighborhood<int32_t>(*s, *params, local_search != 0, nullptr, labels_out, result);
+    ccb_solver& s = CachedSolver(bits, n, words_per_row, edges, 2, batch, params->ls_kernel);
+    if (s.plan.wide) {
+      RunNeighborhood<int32_t>(s, *params, local_search != 0, nullptr, labels_out, result);
     } else {
-      RunNeighborhood<int16_t>(*s, *params, local_search != 0, nullptr, labels_out, result);
+      RunNeighborhood<int16_t>(s, *params, local_search != 0, nullptr, labels_out, result);
     }
     result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
   });

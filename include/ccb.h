@@ -87,6 +87,13 @@ int ccb_neighborhood_solve(const uint32_t* bits, uint32_t n, uint32_t words_per_
                            const ccb_params* params, int32_t local_search, int32_t* labels_out,
                            ccb_result* result);
 
+/* The two one-call entry points above keep, per calling host thread, the device buffers of their last call
+ * (graph rows, population, scratch) and reuse them when the next call on the same device has the same n, k,
+ * population and ls_kernel: a repeated solve then pays the bitset upload, not the allocations.  No
+ * counterpart in the reference, whose calls allocate and free everything (cuda/cc_pbils_gpu.cu:105-122).
+ * ccb_release_cache frees the calling thread's buffers; they are also freed when the thread exits. */
+void ccb_release_cache(void);
+
 /* ---- device-resident graphs and reusable solvers ----------------------------------------------
  * The reference uploads the graph and allocates the population inside every solve
  * (cuda/cc_pbils_gpu.cu:186-226).  These split that constructor so that a caller can keep the graph

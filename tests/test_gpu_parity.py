@@ -260,3 +260,17 @@ def test_solvers_sharing_a_kernel_keep_their_shared_memory(ccb, oracle, cuda_dev
     want = oracle.pbils(big_bits, big_e, make_params(k=5, population=8, iterations=2))
     _same(big.pbils(p), want)
     _same(small.pbils(p), oracle.pbils(small_bits, small_e, make_params(k=5, population=8, iterations=2)))
+
+
+def test_one_call_cache_reuses_buffers_exactly(ccb, oracle, cuda_device):
+    """Repeated one-call solves of the same shape reuse the cached device buffers (a new bitset each time);
+    every result equals the oracle's, also after the cache is released and for a different graph."""
+    p = dict(k=4, population=16, iterations=5, seed=2)
+    for graph_seed in (3, 4, 3):
+        bits, edges = oracle.erdos_renyi(500, 0.3, graph_seed)
+        want = oracle.pbils(bits, edges, make_params(**p))
+        _same(ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, **p)), want, graph_seed)
+    ccb.lib().ccb_release_cache()
+    bits, edges = oracle.erdos_renyi(500, 0.3, 4)
+    _same(ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, **p)),
+          oracle.pbils(bits, edges, make_params(**p)), "after release")
