@@ -1257,20 +1257,47 @@ struct ccb_server {
   size_t in_use = 0;
   int next_id = 0;
   std::deque<Request> queue;
-  std::vector<Active> active;  // entry order of the device table
+  // Requests in the batched iterations run in lanes by size (n <= 2048, n <= 8192, larger).  Each lane steps
+  // on a stream of its own, so while a lane of large requests runs one iteration, a lane of small ones runs
+  // many, and small requests finish in the time their own work takes.
+  struct Lane {
+    std::vector<Active> active;  // entry order of the lane's device table
+    WorkLists work;
+    BatchEntry* d_entries = nullptr;
+    size_t entries_cap = 0;
+    int32_t* d_active = nullptr;
+    int32_t* d_stops = nullptr;
+    int32_t* h_stops = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    bool dirty = true;
+    bool in_flight = false;
+    int launched = 0;  // entries of the iteration in flight (later admissions are appended behind them)
+    ~Lane() {
+      if (stream) cudaStreamSynchronize(stream);
+      active.clear();
+      if (d_entries) cudaFree(d_entries);
+      if (d_active) cudaFree(d_active);
+      if (d_stops) cudaFree(d_stops);
+      if (h_stops) cudaFreeHost(h_stops);
+      if (done) cudaEventDestroy(done);
+      if (stream) cudaStreamDestroy(stream);
+    }
+  };
+  static constexpr int kLanes = 3;
+  Lane lanes[kLanes];
   std::unordered_map<int, Done> done;
-  WorkLists work;
-  BatchEntry* d_entries = nullptr;
-  size_t entries_cap = 0;
-  int32_t* d_active = nullptr;
-  int32_t* d_stops = nullptr;
-  int32_t* h_stops = nullptr;
-  size_t stops_cap = 0;
-  cudaStream_t stream = nullptr;
-  bool dirty = true;
+  cudaStream_t stream = nullptr;  // admission: graph upload or generation, solver initialisation
   long long steps = 0;
   std::vector<std::unique_ptr<Side>> sides;
   int max_sides = 4;
+
+  static int LaneOf(uint32_t n) { return n <= 2048 ? 0 : (n <= 8192 ? 1 : 2); }
+  int ActiveCount() const {
+    size_t c = sides.size();
+    for (const Lane& l : lanes) c += l.active.size();
+    return (int)c;
+  }
 
   ~ccb_server() {
     for (auto& sd : sides) {
@@ -1278,11 +1305,9 @@ struct ccb_server {
       if (sd->stream) cudaStreamDestroy(sd->stream);
     }
     sides.clear();
-    active.clear();
-    if (d_entries) cudaFree(d_entries);
-    if (d_active) cudaFree(d_active);
-    if (d_stops) cudaFree(d_stops);
-    if (h_stops) cudaFreeHost(h_stops);
+    for (Lane& l : lanes) {
+      if (l.stream) cudaStreamSynchronize(l.stream);
+    }
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1382,9 +1407,10 @@ bool BatchedKernelsTake(const ccb_server& sv, const ccb_server::Request& r) {
 // larger than the whole budget is admitted alone.  Requests the batched kernels do not take (n = 0, k = 1,
 // n > 32767) are solved on admission on the plain path.
 void Admit(ccb_server& sv) {
-  while (!sv.queue.empty() && (int)sv.active.size() < sv.max_active) {
+  bool admitted = false;
+  while (!sv.queue.empty() && sv.ActiveCount() < sv.max_active) {
     ccb_server::Request& r = sv.queue.front();
-    if (sv.in_use + r.bytes > sv.budget && !(sv.active.empty() && sv.sides.empty())) break;
+    if (sv.in_use + r.bytes > sv.budget && sv.ActiveCount() > 0) break;
     if ((int)sv.sides.size() >= sv.max_sides && r.n > 0 && !BatchedKernelsTake(sv, r)) break;
     ccb_server::Active a;
     a.admitted = std::chrono::steady_clock::now();
@@ -1419,15 +1445,76 @@ void Admit(ccb_server& sv) {
     }
     EnqueueInit(*a.solver, q.params, sv.stream);
     sv.in_use += q.bytes;
-    sv.active.push_back(std::move(a));
-    sv.dirty = true;
+    ccb_server::Lane& lane = sv.lanes[ccb_server::LaneOf(q.n)];
+    lane.active.push_back(std::move(a));
+    lane.dirty = true;
+    admitted = true;
+  }
+  // the lanes' streams read what admission wrote on its stream
+  if (admitted) CCB_CUDA(cudaStreamSynchronize(sv.stream));
+}
+
+// One iteration of every request of the lane, enqueued on the lane's stream (its device table and work lists
+// rebuilt first if its set of requests changed); the stop flags come back to pinned memory behind it.
+void LaunchLane(ccb_server::Lane& L, const Device& device) {
+  const int count = (int)L.active.size();
+  if (L.dirty) {
+    std::vector<BatchEntry> entries;
+    std::vector<const ccb_solver*> solvers;
+    for (ccb_server::Active& a : L.active) {
+      entries.push_back(MakeEntry(*a.solver, a.req.params));
+      solvers.push_back(a.solver.get());
+    }
+    if ((size_t)count > L.entries_cap) {
+      if (L.d_entries) cudaFree(L.d_entries);
+      if (L.d_stops) cudaFree(L.d_stops);
+      if (L.h_stops) cudaFreeHost(L.h_stops);
+      L.entries_cap = std::max<size_t>(count, 2 * L.entries_cap);
+      CCB_CUDA(cudaMalloc(&L.d_entries, L.entries_cap * sizeof(BatchEntry)));
+      CCB_CUDA(cudaMalloc(&L.d_stops, L.entries_cap * sizeof(int32_t)));
+      CCB_CUDA(cudaMallocHost(&L.h_stops, L.entries_cap * sizeof(int32_t)));
+    }
+    CCB_CUDA(cudaMemcpyAsync(L.d_entries, entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
+                             L.stream));
+    CCB_CUDA(cudaStreamSynchronize(L.stream));
+    BuildWorkLists(L.work, solvers, device, 0.0);
+    L.dirty = false;
+  }
+  EnqueueIteration(L.work, L.d_entries, count, L.d_active, L.d_stops, L.stream);
+  CCB_CUDA(cudaMemcpyAsync(L.h_stops, L.d_stops, count * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream));
+  CCB_CUDA(cudaEventRecord(L.done, L.stream));
+  L.in_flight = true;
+  L.launched = count;
+}
+
+// After the lane's iteration completed: results of the requests that stopped, their memory back to the budget.
+void RetireLane(ccb_server& sv, ccb_server::Lane& L, std::vector<int>& finished) {
+  L.in_flight = false;
+  for (int e = L.launched - 1; e >= 0; --e) {
+    if (!L.h_stops[e]) continue;
+    ccb_server::Active& a = L.active[e];
+    ccb_solver& s = *a.solver;
+    std::vector<int32_t> labels(s.n);
+    CopyOutLabels(s, labels.data(), L.stream);
+    const Control& c = s.host_ctl[0];
+    if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+    ccb_result r{};
+    r.objective = c.record_f;
+    r.iterations_done = c.iterations_done;
+    r.local_searches = (int64_t)c.iterations_done * s.pop;
+    r.accepted_moves = (int64_t)c.moves;
+    r.clusters_used = CountClustersUsed(labels.data(), (uint32_t)s.n, s.k);
+    Finish(sv, a, r, std::move(labels));
+    finished.push_back(a.req.id);
+    sv.in_use -= a.req.bytes;
+    L.active.erase(L.active.begin() + e);
+    L.dirty = true;
   }
 }
 
 void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t* finished_count) {
   const size_t done_before = sv.done.size();
   std::vector<int> newly;
-  auto note = [&](int id) { newly.push_back(id); };
   // ids finished on the plain path during admission
   std::vector<int> before_ids;
   before_ids.reserve(sv.done.size());
@@ -1439,57 +1526,29 @@ void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t
     for (const auto& kv : sv.done)
       if (!std::binary_search(before_ids.begin(), before_ids.end(), kv.first) &&
           std::find(newly.begin(), newly.end(), kv.first) == newly.end())
-        note(kv.first);
+        newly.push_back(kv.first);
   }
-  const int count = (int)sv.active.size();
-  if (count == 0 && !sv.sides.empty()) std::this_thread::sleep_for(std::chrono::microseconds(200));
-  if (count > 0) {
-    if (sv.dirty) {
-      std::vector<BatchEntry> entries;
-      std::vector<const ccb_solver*> solvers;
-      for (ccb_server::Active& a : sv.active) {
-        entries.push_back(MakeEntry(*a.solver, a.req.params));
-        solvers.push_back(a.solver.get());
+  bool any = false;
+  for (ccb_server::Lane& L : sv.lanes) {
+    if (!L.in_flight && !L.active.empty()) LaunchLane(L, sv.device);
+    any |= L.in_flight;
+  }
+  if (any) {
+    // wait until at least one lane finished its iteration (bounded: every kernel of an iteration ends)
+    for (bool got = false; !got;) {
+      for (ccb_server::Lane& L : sv.lanes) {
+        if (!L.in_flight) continue;
+        const cudaError_t q = cudaEventQuery(L.done);
+        if (q == cudaErrorNotReady) continue;
+        CCB_CUDA(q);
+        RetireLane(sv, L, newly);
+        got = true;
       }
-      if ((size_t)count > sv.entries_cap) {
-        if (sv.d_entries) cudaFree(sv.d_entries);
-        if (sv.d_stops) cudaFree(sv.d_stops);
-        if (sv.h_stops) cudaFreeHost(sv.h_stops);
-        sv.entries_cap = std::max<size_t>(count, 2 * sv.entries_cap);
-        CCB_CUDA(cudaMalloc(&sv.d_entries, sv.entries_cap * sizeof(BatchEntry)));
-        CCB_CUDA(cudaMalloc(&sv.d_stops, sv.entries_cap * sizeof(int32_t)));
-        CCB_CUDA(cudaMallocHost(&sv.h_stops, sv.entries_cap * sizeof(int32_t)));
-      }
-      CCB_CUDA(cudaMemcpyAsync(sv.d_entries, entries.data(), count * sizeof(BatchEntry), cudaMemcpyHostToDevice,
-                               sv.stream));
-      CCB_CUDA(cudaStreamSynchronize(sv.stream));
-      BuildWorkLists(sv.work, solvers, sv.device, 0.0);
-      sv.dirty = false;
+      if (!got) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
-    EnqueueIteration(sv.work, sv.d_entries, count, sv.d_active, sv.d_stops, sv.stream);
-    CCB_CUDA(cudaMemcpyAsync(sv.h_stops, sv.d_stops, count * sizeof(int32_t), cudaMemcpyDeviceToHost, sv.stream));
-    CCB_CUDA(cudaStreamSynchronize(sv.stream));
     ++sv.steps;
-    for (int e = count - 1; e >= 0; --e) {
-      if (!sv.h_stops[e]) continue;
-      ccb_server::Active& a = sv.active[e];
-      ccb_solver& s = *a.solver;
-      std::vector<int32_t> labels(s.n);
-      CopyOutLabels(s, labels.data(), sv.stream);
-      const Control& c = s.host_ctl[0];
-      if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
-      ccb_result r{};
-      r.objective = c.record_f;
-      r.iterations_done = c.iterations_done;
-      r.local_searches = (int64_t)c.iterations_done * s.pop;
-      r.accepted_moves = (int64_t)c.moves;
-      r.clusters_used = CountClustersUsed(labels.data(), (uint32_t)s.n, s.k);
-      Finish(sv, a, r, std::move(labels));
-      note(a.req.id);
-      sv.in_use -= a.req.bytes;
-      sv.active.erase(sv.active.begin() + e);
-      sv.dirty = true;
-    }
+  } else if (!sv.sides.empty()) {
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
   }
   if (finished_count) *finished_count = (int32_t)newly.size();
   if (finished_ids) {
@@ -1694,7 +1753,11 @@ int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server*
     sv->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : free_b * 8 / 10;
     sv->max_active = max_active > 0 ? max_active : 1024;
     CCB_CUDA(cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking));
-    CCB_CUDA(cudaMalloc(&sv->d_active, sizeof(int32_t)));
+    for (ccb_server::Lane& L : sv->lanes) {
+      CCB_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+      CCB_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+      CCB_CUDA(cudaMalloc(&L.d_active, sizeof(int32_t)));
+    }
     *out = sv.release();
   });
 }
@@ -1743,7 +1806,7 @@ int ccb_server_status(const ccb_server* sv, int32_t* queued, int32_t* active, ui
   return Guard([&] {
     if (!sv) Fail(CCB_ERR_STATE, "null server");
     if (queued) *queued = (int32_t)sv->queue.size();
-    if (active) *active = (int32_t)(sv->active.size() + sv->sides.size());
+    if (active) *active = (int32_t)sv->ActiveCount();
     if (bytes_in_use) *bytes_in_use = (uint64_t)sv->in_use;
   });
 }

@@ -191,11 +191,14 @@ int ccb_tuning_get(ccb_tuning_entry* entries, int32_t capacity, int32_t* count);
 /* ---- serving ------------------------------------------------------------------------------------
  * No counterpart in the reference.  A request loop with continuous batching: submitted requests wait in a
  * FIFO queue; every ccb_server_step admits queued requests while their estimated device memory (graph rows
- * + population buffers) fits the budget, runs ONE PBILS iteration for every admitted request together (the
- * batched bucket kernels; each request keeps its own iteration count, so requests admitted at different
- * steps interleave on the device), and retires the finished ones, freeing their memory for the queue.
- * Each result equals the request's plain solve.  Requests the batched kernels do not take (k = 1,
- * n > 32767) are solved on the plain path when admitted.  Not thread-safe: one host thread drives a server. */
+ * + population buffers) fits the budget, and advances the admitted ones with the batched bucket kernels.
+ * Admitted requests run in three lanes by size (n <= 2048, n <= 8192, larger), each stepping one PBILS
+ * iteration of all its requests at a time on a stream of its own, so the lanes overlap on the device and a
+ * small request is not held to the pace of a large one; requests admitted later join their lane at its next
+ * iteration.  A step launches every idle lane, waits until at least one lane finished its iteration, and
+ * retires the requests that stopped, freeing their memory for the queue.  Each result equals the request's
+ * plain solve.  Requests the batched kernels do not take (k = 1, n > 32767) run their plain solve on a host
+ * thread of their own, overlapping the lanes.  Not thread-safe: one host thread drives a server. */
 typedef struct ccb_server ccb_server;
 /* hbm_budget_bytes 0: 80% of the free device memory; max_active 0: 1024. */
 int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server** out);
@@ -207,8 +210,8 @@ int ccb_server_submit(ccb_server* server, const uint32_t* bits, uint32_t n, uint
 int ccb_server_submit_generated(ccb_server* server, int32_t planted, uint32_t n, double density_or_p_in,
                                 double p_out, double flip, int32_t parts, uint64_t graph_seed,
                                 const ccb_params* params, int32_t* id_out);
-/* Admission, one iteration of every active request, retirement.  Writes the ids finished in this step (up
- * to capacity) and their count.  Synchronous. */
+/* Admission, an iteration of every idle lane, retirement (see above).  Writes the ids finished in this step
+ * (up to capacity) and their count.  Returns after at least one lane finished an iteration. */
 int ccb_server_step(ccb_server* server, int32_t* finished_ids, int32_t capacity, int32_t* finished_count);
 int ccb_server_status(const ccb_server* server, int32_t* queued, int32_t* active, uint64_t* bytes_in_use);
 /* done = 1 and the result (labels: n int32) once request `id` finished; the result is then released. */

@@ -113,7 +113,8 @@ def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
     """Requests served together with others, admitted at different steps under a tight memory budget and
     a small active cap, give exactly the result of the same request served alone and of its plain solve."""
     reqs = []
-    for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(MIX):
+    lanes = MIX + [(9000, 12, 4, 0.1, 5, 2, 6, 0.4, 21), (3000, 20, 8, 0.1, 5, 3, 6, 0.4, 22)]
+    for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(lanes):
         host, _ = ccb.Graph.Planted(n, max(2, k // 2), 0.5, 0.05, 0.1, 200 + i)
         p = ccb.PbilsParams(k=k, population=pop, gww=gww, tournament=tour, iterations=iters, early_stop=early,
                             perturbation=pert, seed=seed)
