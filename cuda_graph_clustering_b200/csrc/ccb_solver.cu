@@ -1257,7 +1257,7 @@ struct ccb_server {
   size_t in_use = 0;
   int next_id = 0;
   std::deque<Request> queue;
-  // Requests in the batched iterations run in lanes by size (n <= 2048, n <= 8192, larger).  Each lane steps
+  // Requests in the batched iterations run in lanes by size (n <= 1024, 2048, 4096, 8192, larger).  Each lane steps
   // on a stream of its own, so while a lane of large requests runs one iteration, a lane of small ones runs
   // many, and small requests finish in the time their own work takes.
   struct Lane {
@@ -1284,7 +1284,7 @@ struct ccb_server {
       if (stream) cudaStreamDestroy(stream);
     }
   };
-  static constexpr int kLanes = 3;
+  static constexpr int kLanes = 5;
   Lane lanes[kLanes];
   std::unordered_map<int, Done> done;
   cudaStream_t stream = nullptr;  // admission: graph upload or generation, solver initialisation
@@ -1292,7 +1292,7 @@ struct ccb_server {
   std::vector<std::unique_ptr<Side>> sides;
   int max_sides = 4;
 
-  static int LaneOf(uint32_t n) { return n <= 2048 ? 0 : (n <= 8192 ? 1 : 2); }
+  static int LaneOf(uint32_t n) { return n <= 1024 ? 0 : n <= 2048 ? 1 : n <= 4096 ? 2 : n <= 8192 ? 3 : 4; }
   int ActiveCount() const {
     size_t c = sides.size();
     for (const Lane& l : lanes) c += l.active.size();

@@ -192,7 +192,7 @@ int ccb_tuning_get(ccb_tuning_entry* entries, int32_t capacity, int32_t* count);
  * No counterpart in the reference.  A request loop with continuous batching: submitted requests wait in a
  * FIFO queue; every ccb_server_step admits queued requests while their estimated device memory (graph rows
  * + population buffers) fits the budget, and advances the admitted ones with the batched bucket kernels.
- * Admitted requests run in three lanes by size (n <= 2048, n <= 8192, larger), each stepping one PBILS
+ * Admitted requests run in five lanes by size (n <= 1024, 2048, 4096, 8192, larger), each stepping one PBILS
  * iteration of all its requests at a time on a stream of its own, so the lanes overlap on the device and a
  * small request is not held to the pace of a large one; requests admitted later join their lane at its next
  * iteration.  A step launches every idle lane, waits until at least one lane finished its iteration, and
