@@ -87,27 +87,24 @@ __device__ __forceinline__ bool FoldMove(int u, int kf, int kt, int from, int to
     return true;
   }
   const int own = ko & 63;
-  if (own == from) ko = kf;
-  if (own == to) ko = kt;
-  const int b = kb == 0x7fffffff ? -1 : (kb & 63);
-  int m1 = (b == from || b == to) ? 0x7fffffff : kb;  // known keys: the cached best if unchanged,
-  int m2 = 0x7fffffff;
-  if (own != from && !from_empty) {                   // key_from if it is foreign and non-empty,
-    m2 = min(m2, max(m1, kf));
-    m1 = min(m1, kf);
-  }
-  if (own != to) {                                    // key_to if it is foreign
-    m2 = min(m2, max(m1, kt));
-    m1 = min(m1, kt);
-  }
-  if (m1 < lb) {
-    kb = m1;
-    lb = min(lb, m2);
+  const bool of = own == from, ot = own == to;
+  ko = of ? kf : (ot ? kt : ko);
+  // known keys: the cached best if its cluster is neither from nor to (kb = INT_MAX, no best, reads as
+  // cluster 63 and stays INT_MAX either way), key_from if foreign and non-empty, key_to if foreign
+  const int b = kb & 63;
+  const int m1 = (b == from || b == to) ? 0x7fffffff : kb;
+  const int cf = (of || from_empty) ? 0x7fffffff : kf;
+  const int ct = ot ? 0x7fffffff : kt;
+  const int lo = min(cf, ct), hi = max(cf, ct);
+  const int n1 = min(m1, lo);
+  const int n2 = min(max(m1, lo), hi);  // second smallest of the three
+  if (n1 < lb) {
+    kb = n1;
+    lb = min(lb, n2);
     return false;
   }
   return true;
 }
-
 // Shared or global layout of one slot's incremental state (all arrays indexed by vertex, leading dimension ld).
 struct IncState {
   uint16_t* g;    // [k][ld] counters G_c(u), cluster-major: the two lanes a move touches are contiguous
@@ -427,6 +424,7 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
     uint32_t payload = 0;
     const int offf = pending ? off[from] : 0;
     const int offt = pending ? off[to] : 0;
+    const int empty_key = empty >= 0 ? empty : 0x7fffffff;
     // with the keys in shared memory nothing is indexed by j in registers: one group body, looped
 #pragma unroll(kSmemKeys ? 1 : V / kGroup)
     for (int j0 = 0; j0 < V; j0 += kGroup) {
@@ -449,7 +447,7 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
           cko[i] = sko[(j0 + i) * T + tid];
         }
       }
-      unsigned need = 0, chg = 0;  // bit i: rescan needed / cached keys changed
+      unsigned need = 0;  // bit i: rescan needed
       if (pending) {
 #pragma unroll
         for (int i = 0; i < kGroup; ++i) {
@@ -463,11 +461,9 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
             g[static_cast<size_t>(from) * ld + u] = static_cast<uint16_t>(--gf[i]);
             g[static_cast<size_t>(to) * ld + u] = static_cast<uint16_t>(++gt[i]);
           }
-          const int kb0 = kbj, lb0 = lbj, ko0 = koj;
           if (FoldMove(u, offf - 128 * gf[i], offt - 128 * gt[i], from, to, moved, from_empty, kbj, lbj, koj)) {
             need |= 1u << i;
           }
-          chg |= static_cast<unsigned>(kbj != kb0 || lbj != lb0 || koj != ko0) << i;
         }
         // warp-cooperative rescans, one vertex at a time
 #pragma unroll
@@ -498,13 +494,13 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
         const int lbj = kSmemKeys ? clb[i] : lbr[kSmemKeys ? 0 : j];
         const int koj = kSmemKeys ? cko[i] : ko[kSmemKeys ? 0 : j];
         if constexpr (kSmemKeys) {
-          if ((chg | need) >> i & 1u) {
+          if (pending) {  // cheaper than testing what changed: the three words are this thread's own
             skb[j * T + tid] = kbj;
             slb[j * T + tid] = lbj;
             sko[j * T + tid] = koj;
           }
         }
-        const int kbest = min(kbj, empty >= 0 ? empty : 0x7fffffff);
+        const int kbest = min(kbj, empty_key);
         const int gain = (kbest >> 6) - (koj >> 6) + 1;
         const uint32_t mk = static_cast<uint32_t>(gain * (1 << bits)) + key_base + static_cast<uint32_t>(u);
         if (mk < best) {
