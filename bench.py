@@ -10,12 +10,16 @@ Metric: PBILS iterations per second over the whole job (all ranks), plus LS move
 `value`: device time (CUDA events on the solver's stream) of solves on a graph and buffers already
 resident in HBM; L2 is flushed (a 256 MiB write) between timed steps, outside the events.
 `e2e`: the one-call public C ABI (ccb_pbils_solve) from a pinned host bitset to host labels, wall
-clock, every step paying the upload, allocation and the label read-back.
+clock, every step paying the bitset upload, the degree count and the label read-back (the library keeps
+its device buffers across one-call solves of the same shape, so only the first call allocates).
 Every step's objective is checked against the value the CPU oracle gives for this instance.
 
+Other workloads: north (G(32000, 0.33), k=8), wide2 / wide3 (G(65536, 0.02), k=2 / 3), batched (the
+256-instance mix, batched engine vs plain path), serving (Poisson request stream, server vs plain FIFO).
+
 Multi-GPU (torchrun): each rank solves its own instance (a different search seed) with no
-collective on the data path ("scaling": "weak"); the only collectives are the timing barrier and
-the max over ranks.
+collective on the data path ("scaling": "weak"); the only collectives are the timing barrier, the
+max over ranks of the times and the sum of the counts (combine_over_ranks).
 """
 from __future__ import annotations
 
@@ -190,6 +194,20 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def combine_over_ranks(dist, maxes, sums, device="cuda"):
+    """The replicas' only collectives: the max over ranks of the times, the sum over ranks of the counts.
+    Returns (maxes, sums) as lists of floats; without a process group the inputs come back unchanged."""
+    import torch
+
+    if dist is None:
+        return [float(x) for x in maxes], [float(x) for x in sums]
+    mx = torch.tensor([float(x) for x in maxes], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(x) for x in sums], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
 def percentile(xs, q):
     xs = sorted(xs)
     return xs[min(len(xs) - 1, int(math.ceil(q * len(xs))) - 1)] if xs else None
@@ -260,10 +278,7 @@ def run_batched(args, rank, world, local):
     barrier()
     tb = max(t_batch)
     tp = sum(t_plain)
-    vals = torch.tensor([tb, tp], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    tb_all, tp_all = vals[0].item(), vals[1].item()
+    (tb_all, tp_all), _ = combine_over_ranks(dist, [tb, tp], [])
     if rank == 0:
         count = len(mix)
         done = []
@@ -387,10 +402,7 @@ def run_serving(args, rank, world, local):
         free_at = max(free_at, arr) + sdur
         fifo.append(free_at)
     t_fifo = fifo[-1]
-    vals = torch.tensor([t_serve, t_fifo], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ts_all, tf_all = vals[0].item(), vals[1].item()
+    (ts_all, tf_all), _ = combine_over_ranks(dist, [t_serve, t_fifo], [])
     if rank == 0:
         lat_s = [finish[j] - reqs[j][0] for j in range(len(reqs))]
         lat_f = [fifo[j] - reqs[j][0] for j in range(len(reqs))]
@@ -527,15 +539,7 @@ def main():
         bit_exact = recount_ok and all(r.objective == results[0].objective for r in results)
 
     # ---- max over ranks ------------------------------------------------------------------------
-    vals = torch.tensor([total_ms, e2e_s, float(iters), float(moves)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        mx = vals.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = vals.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_ms_all, e2e_all, iters_all, moves_all = mx[0].item(), mx[1].item(), sm[2].item(), sm[3].item()
-    else:
-        total_ms_all, e2e_all, iters_all, moves_all = total_ms, e2e_s, float(iters), float(moves)
+    (total_ms_all, e2e_all), (iters_all, moves_all) = combine_over_ranks(dist, [total_ms, e2e_s], [iters, moves])
 
     if rank == 0:
         n, k, pop = cfg["n"], cfg["k"], cfg["population"]
