@@ -1417,33 +1417,42 @@ void Admit(ccb_server& sv) {
     a.req = std::move(r);
     sv.queue.pop_front();
     const ccb_server::Request& q = a.req;
-    if (q.source == 0) {
-      a.graph.reset(MakeGraph(q.bits.data(), false, q.n, q.words, q.edges, sv.stream));
-      a.req.bits.clear();
-      a.req.bits.shrink_to_fit();
-    } else {
-      ccb_graph* g = nullptr;
-      const int status =
-          q.source == 1 ? ccb_graph_generate_erdos_renyi(q.n, q.density, q.graph_seed, sv.stream, &g)
-                        : ccb_graph_generate_planted(q.n, q.parts, 0, q.p_in, q.p_out, q.flip, q.graph_seed, sv.stream,
-                                                     &g, nullptr);
-      if (status != CCB_OK) Fail(status, LastError());
-      a.graph.reset(g);
-    }
-    if (q.n == 0) {
-      ccb_result r0{};
-      EmptyPbils(q.params, &r0);
-      Finish(sv, a, r0, {});
+    try {
+      if (q.source == 0) {
+        a.graph.reset(MakeGraph(q.bits.data(), false, q.n, q.words, q.edges, sv.stream));
+        a.req.bits.clear();
+        a.req.bits.shrink_to_fit();
+      } else {
+        ccb_graph* g = nullptr;
+        const int status =
+            q.source == 1 ? ccb_graph_generate_erdos_renyi(q.n, q.density, q.graph_seed, sv.stream, &g)
+                          : ccb_graph_generate_planted(q.n, q.parts, 0, q.p_in, q.p_out, q.flip, q.graph_seed, sv.stream,
+                                                       &g, nullptr);
+        if (status != CCB_OK) Fail(status, LastError());
+        a.graph.reset(g);
+      }
+      if (q.n == 0) {
+        ccb_result r0{};
+        EmptyPbils(q.params, &r0);
+        Finish(sv, a, r0, {});
+        continue;
+      }
+      a.solver.reset(MakeSolver(a.graph.get(), q.params.k, q.params.population, CCB_LS_AUTO));
+      const Plan& pl = a.solver->plan;
+      if (pl.wide || !(pl.small_k || pl.incremental)) {
+        CCB_CUDA(cudaStreamSynchronize(sv.stream));  // the graph is complete before another stream reads it
+        StartSide(sv, std::move(a));
+        continue;
+      }
+      EnqueueInit(*a.solver, q.params, sv.stream);
+    } catch (const Failure& f) {
+      // the request fails alone (its graph or buffers could not be made): ccb_server_result reports the error
+      ccb_server::Done d;
+      d.status = f.status;
+      d.error = f.message;
+      sv.done[q.id] = std::move(d);
       continue;
     }
-    a.solver.reset(MakeSolver(a.graph.get(), q.params.k, q.params.population, CCB_LS_AUTO));
-    const Plan& pl = a.solver->plan;
-    if (pl.wide || !(pl.small_k || pl.incremental)) {
-      CCB_CUDA(cudaStreamSynchronize(sv.stream));  // the graph is complete before another stream reads it
-      StartSide(sv, std::move(a));
-      continue;
-    }
-    EnqueueInit(*a.solver, q.params, sv.stream);
     sv.in_use += q.bytes;
     ccb_server::Lane& lane = sv.lanes[ccb_server::LaneOf(q.n)];
     lane.active.push_back(std::move(a));

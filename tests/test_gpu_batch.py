@@ -153,3 +153,23 @@ def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
     wg = ccb.DeviceGraph.erdos_renyi(34000, 0.004, 78)
     assert _results_equal(out[wid], ccb.SolveGpu(wg.download(), wp))
     sv.close()
+
+
+def test_server_request_that_cannot_be_admitted_fails_alone(ccb, cuda_device):
+    """A request whose buffers exceed the device memory fails at admission without allocating; its result
+    carries the error and the requests around it are served as usual."""
+    host, _ = ccb.Graph.Planted(1000, 3, 0.5, 0.05, 0.1, 31)
+    small = ccb.PbilsParams(k=6, population=8, iterations=3, seed=4)
+    sv = ccb.Server()
+    bad = sv.submit(host, ccb.PbilsParams(k=64, population=5_000_000, iterations=1))
+    good = sv.submit(host, small)
+    results, errors = {}, {}
+    while len(results) + len(errors) < 2:
+        for i in sv.step():
+            try:
+                results[i] = sv.result(i)
+            except ccb.CcbError as e:
+                errors[i] = e
+    assert set(errors) == {bad} and "device memory" in str(errors[bad])
+    assert _results_equal(results[good], ccb.SolveGpu(host, small))
+    sv.close()
