@@ -74,6 +74,7 @@ struct RebuildArgs {
   float probability;
   int first;
   const Control* ctl;  // checked for the stop flag in the perturb / copy modes (may be null)
+  int64_t* intra = nullptr;  // tiled form: labels, masks and sizes only; intra[slot] zeroed for the tiles
 };
 
 template <typename GainT, int kThreads>
@@ -137,6 +138,11 @@ __device__ __forceinline__ void RebuildBody(const RebuildArgs<GainT>& a, int slo
     }
   }
   __syncthreads();
+  if (a.intra != nullptr) {  // the tiled form computes G and f in k_rebuild_tiles / k_rebuild_finish
+    for (int c = tid; c < k; c += kThreads) cur.sizes[static_cast<size_t>(slot) * kpad + c] = s_sizes[c];
+    if (tid == 0) a.intra[slot] = 0;
+    return;
+  }
 
   // Phase 3: one row per thread.  The row streams in as 16-byte vectors (L1 keeps its line while the
   // thread walks it); every thread of the block reads the same mask vector at the same step, a broadcast.
@@ -186,6 +192,98 @@ __device__ __forceinline__ void RebuildBody(const RebuildArgs<GainT>& a, int slo
 template <typename GainT, int kThreads>
 __global__ void __launch_bounds__(kThreads) k_rebuild(RebuildArgs<GainT> a) {
   RebuildBody<GainT, kThreads>(a, blockIdx.x);
+}
+
+// G = A*Z for every slot with each adjacency row read from memory once per rebuild (the one-block-per-slot
+// form reads all n rows once per slot: at n = 65536 that is 512 MiB per slot).  A block stages a tile of
+// kRows rows (one per warp) in shared memory, then walks the slots: warp w popcounts its row against the
+// slot's cluster masks (read through L1, shared by the block's warps), writes G_c of its vertex for
+// c < k - 1, derives G_{k-1} from the degree, and adds G_own to the slot's intra sum (one atomic per block
+// and slot).  Runs after k_rebuild in its tiled form (labels, masks, sizes); k_rebuild_finish turns the
+// intra sums into f.
+struct RebuildTilesArgs {
+  GraphView gr;
+  const uint8_t* labels;  // [slot][ld]
+  const uint32_t* masks;  // [slot][k][pitch]
+  int32_t* g;             // [slot][k][ld]
+  int64_t* intra;         // [slot]
+  int count, k, ld;
+  int mode;
+  const Control* ctl;
+};
+
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1) k_rebuild_tiles(RebuildTilesArgs a) {
+  constexpr int kRows = kThreads / kWarp;
+  extern __shared__ __align__(16) uint4 s_rows[];  // kRows x pitch words
+  __shared__ long long s_part[kRows];
+  if (a.ctl != nullptr && (a.mode == kRebuildPerturb || a.mode == kRebuildCopy) && a.ctl->stop) return;
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int warp = tid / kWarp;
+  const int n = a.gr.n;
+  const int pitch = a.gr.pitch;
+  const int quads = pitch / 4;
+  const int r0 = blockIdx.x * kRows;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.gr.bits) + static_cast<size_t>(r0) * quads;
+    const int total = kRows * quads;
+    for (int i = tid; i < total; i += kThreads) {
+      const int row = r0 + i / quads;
+      s_rows[i] = row < n ? src[i] : make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+  __syncthreads();
+  const int v = r0 + warp;
+  const uint4* row = s_rows + static_cast<size_t>(warp) * quads;
+  const int degree = v < n ? a.gr.degrees[v] : 0;
+  for (int slot = 0; slot < a.count; ++slot) {
+    long long own_g = 0;
+    if (v < n) {
+      const int own = a.labels[static_cast<size_t>(slot) * a.ld + v];
+      const uint4* m = reinterpret_cast<const uint4*>(a.masks + static_cast<size_t>(slot) * a.k * pitch);
+      int32_t* g = a.g + static_cast<size_t>(slot) * a.k * a.ld + v;
+      int rest = degree;
+      for (int c = 0; c < a.k - 1; ++c) {
+        int acc = 0;
+        for (int q = lane; q < quads; q += kWarp) {
+          const uint4 r = row[q];
+          const uint4 x = __ldg(m + static_cast<size_t>(c) * quads + q);
+          acc += __popc(r.x & x.x) + __popc(r.y & x.y) + __popc(r.z & x.z) + __popc(r.w & x.w);
+        }
+        acc = __reduce_add_sync(kAllLanes, acc);
+        if (lane == 0) g[static_cast<size_t>(c) * a.ld] = acc;
+        rest -= acc;
+        if (own == c) own_g = acc;
+      }
+      if (lane == 0) g[static_cast<size_t>(a.k - 1) * a.ld] = rest;
+      if (own == a.k - 1) own_g = rest;
+    }
+    if (lane == 0) s_part[warp] = own_g;
+    __syncthreads();
+    if (tid == 0) {
+      long long sum = 0;
+#pragma unroll
+      for (int w = 0; w < kRows; ++w) sum += s_part[w];
+      if (sum != 0) atomicAdd(reinterpret_cast<unsigned long long*>(a.intra + slot), static_cast<unsigned long long>(sum));
+    }
+    __syncthreads();
+  }
+}
+
+// f = m + sum_c C(size_c, 2) - (twice the intra-cluster edges) per slot, after k_rebuild_tiles.
+template <typename GainT>
+__global__ void k_rebuild_finish(PopView<GainT> cur, const int64_t* intra, int count, int k, int kpad, int64_t edges,
+                                 int mode, const Control* ctl) {
+  if (ctl != nullptr && (mode == kRebuildPerturb || mode == kRebuildCopy) && ctl->stop) return;
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= count) return;
+  long long pairs = 0;
+  for (int c = 0; c < k; ++c) {
+    const long long sz = cur.sizes[static_cast<size_t>(slot) * kpad + c];
+    pairs += sz * (sz - 1) / 2;
+  }
+  cur.f[slot] = edges + pairs - intra[slot];
 }
 
 // Steepest descent of one slot per block until no strictly improving single-vertex move remains.

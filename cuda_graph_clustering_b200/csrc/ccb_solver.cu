@@ -50,6 +50,7 @@ namespace {
 
 constexpr int kAuxThreads = 256;
 constexpr int kRebuildThreads = 512;
+constexpr int kRebuildTileThreads = 512;  // 16 rows per tile, one per warp
 constexpr int kRecordThreads = 1024;
 constexpr int kPollChunk = 4;  // iterations enqueued between stop-flag polls
 
@@ -424,6 +425,7 @@ struct ccb_solver {
   int64_t* cur_f = nullptr;
   int64_t* next_f = nullptr;
   uint32_t* masks = nullptr;
+  int64_t* intra = nullptr;    // tiled rebuild (wide path): per-slot intra-cluster sums; null: per-slot rebuild
   int32_t* src_map = nullptr;
   int32_t* order = nullptr;
   uint8_t* record_lab = nullptr;
@@ -516,6 +518,13 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->Alloc(s->cur_f, pop);
   s->Alloc(s->next_f, pop);
   s->Alloc(s->masks, (size_t)pop * k * g->pitch);
+  // Wide graphs do not fit L2: rebuild G with each row read once for all slots (a tile of 16 rows per block in
+  // shared memory) instead of once per slot.
+  if (s->plan.wide && (size_t)kRebuildTileThreads / kWarp * g->pitch * 4 + 2048 <= (size_t)s->device.smem_optin) {
+    s->Alloc(s->intra, pop);
+    CCB_CUDA(RaiseDynamicSmem(k_rebuild_tiles<kRebuildTileThreads>,
+                              (size_t)kRebuildTileThreads / kWarp * g->pitch * 4));
+  }
   s->Alloc(s->src_map, pop);
   s->Alloc(s->order, pop);
   s->Alloc(s->record_lab, s->ld);
@@ -561,8 +570,26 @@ template <typename GainT>
 void LaunchRebuild(ccb_solver& s, int grid, int mode, const int32_t* src_map, uint64_t stream, int iteration,
                    float prob, int first, bool check_stop, cudaStream_t st) {
   if (grid <= 0) return;
-  const RebuildArgs<GainT> a{s.graph->View(), s.Cur<GainT>(), s.next_lab, src_map, s.masks, s.k, s.kpad, s.ld,
-                             mode, stream, iteration, prob, first, check_stop ? s.ctl : nullptr};
+  const Control* ctl = check_stop ? s.ctl : nullptr;
+  RebuildArgs<GainT> a{s.graph->View(), s.Cur<GainT>(), s.next_lab, src_map, s.masks, s.k, s.kpad, s.ld,
+                       mode, stream, iteration, prob, first, ctl};
+  if constexpr (std::is_same_v<GainT, int32_t>) {
+    if (s.intra != nullptr) {
+      a.intra = s.intra;
+      const ccb_graph& g = *s.graph;
+      const RebuildTilesArgs t{g.View(), s.cur_lab, s.masks, s.Cur<int32_t>().g, s.intra, grid, s.k, s.ld, mode, ctl};
+      const int tiles = (g.n + kRebuildTileThreads / kWarp - 1) / (kRebuildTileThreads / kWarp);
+      const size_t smem = (size_t)kRebuildTileThreads / kWarp * g.pitch * 4;
+      s.timer.Time(kCatRebuild, st, [&] {
+        k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(a);
+        k_rebuild_tiles<kRebuildTileThreads><<<tiles, kRebuildTileThreads, smem, st>>>(t);
+        k_rebuild_finish<GainT><<<(grid + 127) / 128, 128, 0, st>>>(s.Cur<GainT>(), s.intra, grid, s.k, s.kpad,
+                                                                    (int64_t)g.edges, mode, ctl);
+      });
+      CCB_CUDA(cudaGetLastError());
+      return;
+    }
+  }
   s.timer.Time(kCatRebuild, st, [&] { k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(a); });
   CCB_CUDA(cudaGetLastError());
 }
