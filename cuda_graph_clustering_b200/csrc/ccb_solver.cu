@@ -1881,10 +1881,11 @@ struct OneCallCache {
   uint32_t n = 0;
   int k = 0, pop = 0, ls = 0;
   void Release() {
-    solver.reset();
+    solver.reset();  // the solver refers to the graph: it goes first
     graph.reset();
     device = -1;
   }
+  ~OneCallCache() { Release(); }
 };
 thread_local OneCallCache t_cache;
 
