@@ -14,7 +14,7 @@ clock, every step paying the bitset upload, the degree count and the label read-
 its device buffers across one-call solves of the same shape, so only the first call allocates).
 Every step's objective is checked against the value the CPU oracle gives for this instance.
 
-Other workloads: north (G(32000, 0.33), k=8), wide2 / wide3 (G(65536, 0.02), k=2 / 3), batched (the
+Other workloads: large (G(32000, 0.33), k=8), wide2 / wide3 (G(65536, 0.02), k=2 / 3), batched (the
 256-instance mix, batched engine vs plain path), serving (Poisson request stream, server vs plain FIFO).
 
 Multi-GPU (torchrun): each rank solves its own instance (a different search seed) with no
@@ -42,7 +42,7 @@ PLAIN = dict(n=1000, density=0.5, graph_seed=1, k=5, population=128, tournament=
 PLAIN_OBJECTIVE = {1: 234911}  # seed -> objective of the CPU oracle (and the reference binary)
 # The large plain configuration of the hot-path roofline target: G(32000, 0.33) from graph seed 7, k=8,
 # pop 128; a step is a short solve (3 iterations) because one iteration costs ~10^4 moves per slot.
-NORTH = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournament=5, perturbation=0.4, gww=0.1,
+LARGE = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournament=5, perturbation=0.4, gww=0.1,
              iterations=3, early_stop=100, seed=1)
 # The wide configuration: G(65536, 0.02) (a 512 MiB bitset) from graph seed 1, k = 2 or 3 on the packed wide
 # descents (int32 G), pop 128, gww 0.1, 50 iterations.  No CPU objective is known at this size: every step's
@@ -50,7 +50,7 @@ NORTH = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournamen
 WIDE2 = dict(n=65536, density=0.02, graph_seed=1, k=2, population=128, tournament=5, perturbation=0.4, gww=0.1,
              iterations=50, early_stop=50, seed=1)
 WIDE3 = dict(WIDE2, k=3)
-WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "north": (NORTH, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {})}
+WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "large": (LARGE, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {})}
 
 
 def parse():
