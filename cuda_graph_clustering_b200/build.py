@@ -1,10 +1,11 @@
 """Builds libccb.so in-tree for sm_100a (B200) with nvcc.
 
-    python -m cuda_graph_clustering_b200.build [--force]
+    python -m cuda_graph_clustering_b200.build [--force] [--cc-gpu]
 
 Every CUDA source is compiled with ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into an
 object under ``cuda_graph_clustering_b200/_build`` and linked into
 ``cuda_graph_clustering_b200/libccb.so``.  Objects are rebuilt only when a source or header is newer.
+With ``--cc-gpu`` it also links the drop-in ``cc_gpu`` binary (the reference's command line on libccb).
 """
 from __future__ import annotations
 
@@ -71,5 +72,34 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+REFERENCE = os.environ.get("CCB_REFERENCE", "/root/reference")
+CC_GPU = os.path.join(PKG, "cc_gpu")
+
+
+def build_cc_gpu(reference: str = REFERENCE, verbose: bool = False) -> str | None:
+    """The drop-in cc_gpu binary: the reference's own command line (include/cc_cli.hpp) and host sources
+    (src/cc_graph.cpp, src/cc_pbils_cpu.cpp), compiled where they lie, linked with cc_gpu_ccb.cpp (the
+    reference's GPU entry points over libccb) and libccb.so.  Returns its path, or None without the reference
+    sources."""
+    inc = os.path.join(reference, "include")
+    srcs = [os.path.join(reference, "src", f) for f in ("cc_graph.cpp", "cc_pbils_cpu.cpp")]
+    if not all(os.path.exists(x) for x in [inc] + srcs):
+        return None
+    lib = build()
+    deps = srcs + [os.path.join(PKG, "cc_gpu_ccb.cpp"), lib, os.path.join(REPO, "include", "ccb.h")]
+    if _stale(CC_GPU, deps):
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-pthread", "-DCCB_CC_GPU_MAIN", "-I", inc,
+               "-I", os.path.join(REPO, "include"), os.path.join(PKG, "cc_gpu_ccb.cpp")] + srcs + \
+              ["-L", PKG, "-lccb", "-Wl,-rpath,$ORIGIN", "-o", CC_GPU]
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"cc_gpu link failed:\n{proc.stderr}")
+        if verbose:
+            print("linked", CC_GPU)
+    return CC_GPU
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    if "--cc-gpu" in sys.argv:
+        print(build_cc_gpu(verbose=True))

@@ -1,6 +1,7 @@
 """The cc_gpu command line mirror: edge-list loading and argument handling on the CPU; a full run on the GPU
 checked against the oracle, with the reference's result-JSON keys and labels file."""
 import json
+import os
 
 import pytest
 
@@ -60,3 +61,38 @@ def test_cli_run_writes_reference_json(tmp_path, oracle, cuda_device, capsys):
     assert r["objective function value"] == best.objective and r["objective max"] == max(x.objective for x in runs)
     assert r["clustering vector"] == [int(x) for x in best.labels]
     assert [int(x) for x in labels.read_text().split()] == [int(x) for x in best.labels]
+
+
+CC_GPU = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "cuda_graph_clustering_b200",
+                      "cc_gpu")
+
+
+def _cc_gpu(*args):
+    import subprocess
+
+    return subprocess.run([CC_GPU, *args], capture_output=True, text=True, timeout=300)
+
+
+@pytest.mark.skipif(not os.path.exists(CC_GPU), reason="drop-in cc_gpu not built (needs the reference sources)")
+def test_drop_in_cc_gpu_rejects_bad_parameters_like_the_reference():
+    """The reference's own command line linked with libccb: parameter errors come back as the reference's
+    messages and exit code before any device work."""
+    r = _cc_gpu("--n", "10", "--k", "65")
+    assert r.returncode == 1 and "error: k exceeds kMaxClusters (64)" in r.stdout
+    r = _cc_gpu("--algorithm", "NeighborhoodCuda", "--n", "10", "--k", "3")
+    assert r.returncode == 1 and "error: Neighborhood algorithms require k = 2" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(CC_GPU), reason="drop-in cc_gpu not built (needs the reference sources)")
+def test_drop_in_cc_gpu_solves_like_the_oracle(tmp_path, oracle, cuda_device):
+    out = tmp_path / "r.json"
+    r = _cc_gpu("--n", "300", "--density", "0.3", "--graph-seed", "4", "--k", "4", "--pop", "16", "--iters", "6",
+                "--out", str(out))
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = json.loads(out.read_text())
+    bits, edges = oracle.erdos_renyi(300, 0.3, 4)
+    want = oracle.pbils(bits, edges, make_params(k=4, population=16, iterations=6, seed=1))
+    assert got["objective function value"] == want.objective
+    assert got["clustering vector"] == [int(x) for x in want.labels]
+    assert got["backend"] == "gpu"
