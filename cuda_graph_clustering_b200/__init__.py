@@ -424,6 +424,13 @@ class Server:
         del self.sizes[i]
         return PbilsResult.from_c(res, labels[:n])
 
+    def cancel(self, i: int) -> bool:
+        """Cancels request i (ccb_server_cancel); its result then raises CcbError with CCB_ERR_CANCELLED.
+        Returns whether the request was found unfinished."""
+        found = C.c_int32()
+        check(lib().ccb_server_cancel(self.handle, i, C.byref(found)))
+        return bool(found.value)
+
     def drain(self) -> dict:
         """Steps until no request is queued or active; returns {id: result} for every request finished."""
         out = {}

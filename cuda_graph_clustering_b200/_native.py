@@ -17,6 +17,7 @@ CCB_ERR_DEVICE_MEMORY = 2
 CCB_ERR_CUDA = 3
 CCB_ERR_TIMEOUT = 4
 CCB_ERR_STATE = 5
+CCB_ERR_CANCELLED = 6
 
 LS_AUTO, LS_GLOBAL, LS_SHARED, LS_WIDE = 0, 1, 2, 3
 MAX_CLUSTERS = 64
@@ -92,6 +93,7 @@ SIGNATURES = {
     "ccb_server_step": (C.c_int, [_vp, _i32p, C.c_int32, C.POINTER(C.c_int32)]),
     "ccb_server_status": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
     "ccb_server_result": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), _vp, C.POINTER(CcbResult)]),
+    "ccb_server_cancel": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32)]),
     "ccb_server_destroy": (None, [_vp]),
     "ccb_evaluate_labelings": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, _vp, _vp,
                                          _vp, _vp, _vp]),

@@ -1262,6 +1262,7 @@ struct ccb_server {
     std::unique_ptr<ccb_graph> graph;
     std::unique_ptr<ccb_solver> solver;
     std::chrono::steady_clock::time_point admitted;
+    bool cancel = false;  // stop it before its lane's next iteration; report CCB_ERR_CANCELLED
   };
   struct Done {
     int status = CCB_OK;
@@ -1405,6 +1406,10 @@ void CollectSides(ccb_server& sv, std::vector<int>& finished) {
     cudaStreamDestroy(sd.stream);
     sd.stream = nullptr;
     sd.out.result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - sd.a.admitted).count();
+    if (sd.a.cancel) {
+      sd.out.status = CCB_ERR_CANCELLED;
+      sd.out.error = "request cancelled";
+    }
     sv.in_use -= sd.a.req.bytes;
     finished.push_back(sd.a.req.id);
     sv.done[sd.a.req.id] = std::move(sd.out);
@@ -1516,6 +1521,12 @@ void LaunchLane(ccb_server::Lane& L, const Device& device) {
     BuildWorkLists(L.work, solvers, device, 0.0);
     L.dirty = false;
   }
+  static const int32_t kStop = 1;
+  for (ccb_server::Active& a : L.active) {
+    if (a.cancel) {  // every kernel of the iteration skips it; the advance reports it stopped
+      CCB_CUDA(cudaMemcpyAsync(&a.solver->ctl->stop, &kStop, sizeof(int32_t), cudaMemcpyHostToDevice, L.stream));
+    }
+  }
   EnqueueIteration(L.work, L.d_entries, count, L.d_active, L.d_stops, L.stream);
   CCB_CUDA(cudaMemcpyAsync(L.h_stops, L.d_stops, count * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream));
   CCB_CUDA(cudaEventRecord(L.done, L.stream));
@@ -1529,6 +1540,17 @@ void RetireLane(ccb_server& sv, ccb_server::Lane& L, std::vector<int>& finished)
   for (int e = L.launched - 1; e >= 0; --e) {
     if (!L.h_stops[e]) continue;
     ccb_server::Active& a = L.active[e];
+    if (a.cancel) {
+      ccb_server::Done d;
+      d.status = CCB_ERR_CANCELLED;
+      d.error = "request cancelled";
+      sv.done[a.req.id] = std::move(d);
+      finished.push_back(a.req.id);
+      sv.in_use -= a.req.bytes;
+      L.active.erase(L.active.begin() + e);
+      L.dirty = true;
+      continue;
+    }
     ccb_solver& s = *a.solver;
     std::vector<int32_t> labels(s.n);
     CopyOutLabels(s, labels.data(), L.stream);
@@ -1864,6 +1886,32 @@ int ccb_server_result(ccb_server* sv, int32_t id, int32_t* done, int32_t* labels
       std::memcpy(labels_out, it->second.labels.data(), it->second.labels.size() * 4);
     }
     sv->done.erase(it);
+  });
+}
+
+int ccb_server_cancel(ccb_server* sv, int32_t id, int32_t* found) {
+  return Guard([&] {
+    if (!sv) Fail(CCB_ERR_STATE, "null server");
+    bool hit = false;
+    for (auto it = sv->queue.begin(); it != sv->queue.end() && !hit; ++it) {
+      if (it->id != id) continue;
+      sv->queue.erase(it);
+      ccb_server::Done d;
+      d.status = CCB_ERR_CANCELLED;
+      d.error = "request cancelled";
+      sv->done[id] = std::move(d);
+      hit = true;
+      break;
+    }
+    for (ccb_server::Lane& L : sv->lanes) {
+      for (ccb_server::Active& a : L.active) {
+        if (!hit && a.req.id == id && !a.cancel) a.cancel = hit = true;
+      }
+    }
+    for (auto& sd : sv->sides) {
+      if (!hit && sd->a.req.id == id && !sd->a.cancel) sd->a.cancel = hit = true;
+    }
+    if (found) *found = hit;
   });
 }
 

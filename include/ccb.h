@@ -30,7 +30,8 @@ enum ccb_status {
   CCB_ERR_DEVICE_MEMORY = 2, /* the run does not fit the free device memory / shared memory */
   CCB_ERR_CUDA = 3,          /* a CUDA runtime call failed */
   CCB_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (batched / serving paths) */
-  CCB_ERR_STATE = 5          /* handle misuse (null handle, queue full, ...) */
+  CCB_ERR_STATE = 5,         /* handle misuse (null handle, queue full, ...) */
+  CCB_ERR_CANCELLED = 6      /* a served request was cancelled (ccb_server_cancel) */
 };
 
 /* PbilsParams::LocalSearchKernel (include/cc_pbils.hpp:27-36). */
@@ -216,6 +217,10 @@ int ccb_server_step(ccb_server* server, int32_t* finished_ids, int32_t capacity,
 int ccb_server_status(const ccb_server* server, int32_t* queued, int32_t* active, uint64_t* bytes_in_use);
 /* done = 1 and the result (labels: n int32) once request `id` finished; the result is then released. */
 int ccb_server_result(ccb_server* server, int32_t id, int32_t* done, int32_t* labels_out, ccb_result* result);
+/* Cancels request `id` (found = 0 if it is unknown or already finished): a queued request leaves the queue, an
+ * admitted one stops before its lane's next iteration and frees its memory when that iteration completes, a
+ * request on a side thread runs to its end and is then dropped.  Its result reports CCB_ERR_CANCELLED. */
+int ccb_server_cancel(ccb_server* server, int32_t id, int32_t* found);
 void ccb_server_destroy(ccb_server* server);
 
 /* ---- device recount -----------------------------------------------------------------------------

@@ -173,3 +173,27 @@ def test_server_request_that_cannot_be_admitted_fails_alone(ccb, cuda_device):
     assert set(errors) == {bad} and "device memory" in str(errors[bad])
     assert _results_equal(results[good], ccb.SolveGpu(host, small))
     sv.close()
+
+
+def test_server_cancel_queued_and_admitted(ccb, cuda_device):
+    """Cancelling a queued request removes it; cancelling an admitted one stops it before its lane's next
+    iteration; both report CCB_ERR_CANCELLED, and the request served after them is unaffected."""
+    host, _ = ccb.Graph.Planted(800, 4, 0.5, 0.05, 0.1, 41)
+    ps = [ccb.PbilsParams(k=5, population=8, iterations=30, early_stop=30, seed=s) for s in (1, 2, 3)]
+    sv = ccb.Server(max_active=1)
+    ids = [sv.submit(host, p) for p in ps]
+    sv.step()  # admits the first request and runs one of its iterations
+    assert sv.cancel(ids[2]) and sv.cancel(ids[0]) and not sv.cancel(123456)
+    results, errors = {}, {}
+    while not (ids[0] in errors and ids[1] in results):
+        for i in sv.step():
+            try:
+                results[i] = sv.result(i)
+            except ccb.CcbError as e:
+                errors[i] = e
+    assert errors[ids[0]].status == ccb._native.CCB_ERR_CANCELLED
+    with pytest.raises(ccb.CcbError) as queued:
+        sv.result(ids[2])
+    assert queued.value.status == ccb._native.CCB_ERR_CANCELLED
+    assert _results_equal(results[ids[1]], ccb.SolveGpu(host, ps[1]))
+    sv.close()
