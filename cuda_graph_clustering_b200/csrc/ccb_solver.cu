@@ -472,6 +472,7 @@ struct ccb_solver {
 namespace {
 
 ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
+  TraceRange trace_range("ccb.solver.create");
   std::unique_ptr<ccb_solver> s(new ccb_solver());
   s->graph = g;
   s->device = Device::Current();
@@ -659,6 +660,7 @@ void PrintPlan(const ccb_solver& s, size_t free_hint) {
 
 template <typename GainT>
 void RunPbils(ccb_solver& s, const ccb_params& p, cudaStream_t st, int32_t* labels_out, ccb_result* res) {
+  TraceRange trace_range("ccb.pbils");
   const auto started = std::chrono::steady_clock::now();
   const int n = s.n, k = s.k, pop = s.pop;
   const uint64_t init_stream = StreamSeed(p.seed, kInitTag, 0);
@@ -753,6 +755,7 @@ void RunPbils(ccb_solver& s, const ccb_params& p, cudaStream_t st, int32_t* labe
 template <typename GainT>
 void RunNeighborhood(ccb_solver& s, const ccb_params& p, bool local_search, cudaStream_t st, int32_t* labels_out,
                      ccb_result* res) {
+  TraceRange trace_range("ccb.neighborhood");
   const auto started = std::chrono::steady_clock::now();
   const int n = s.n;
   const int capacity = std::min(s.pop, n);
@@ -1188,6 +1191,7 @@ void EnqueueInit(ccb_solver& s, const ccb_params& p, cudaStream_t st) {
 }
 
 void RunBatch(ccb_batch& b) {
+  TraceRange trace_range("ccb.batch.run");
   const auto started = std::chrono::steady_clock::now();
   PrepareBatch(b);
   const cudaStream_t st = b.stream;
@@ -1571,6 +1575,7 @@ void RetireLane(ccb_server& sv, ccb_server::Lane& L, std::vector<int>& finished)
 }
 
 void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t* finished_count) {
+  TraceRange trace_range("ccb.server.step");
   const size_t done_before = sv.done.size();
   std::vector<int> newly;
   // ids finished on the plain path during admission

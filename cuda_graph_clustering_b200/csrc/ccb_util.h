@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <new>
 #include <stdexcept>
@@ -12,6 +13,15 @@
 #include "ccb_error.h"
 
 namespace ccb {
+
+// NVTX range over a host-side phase (solve, batch run, server step, solver set-up): visible in Nsight
+// timelines, a no-op when no tool is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 struct Failure {
   int status;
