@@ -165,6 +165,13 @@ def reference_cpu_run(cfg, iterations, threads=0):
     return t, f, threads_used
 
 
+def workload_text(name, cfg):
+    """The `config.workload` string of a PBILS workload, shared by both arms."""
+    return (f"{name} PBILS: ER(n={cfg['n']}, p={cfg['density']}, graph seed {cfg['graph_seed']}), k={cfg['k']}, "
+            f"pop={cfg['population']}, tournament 5, perturb 0.4, gww 0.1, {cfg['iterations']} iterations "
+            f"(early stop off), seed {cfg['seed']} + rank")
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's CPU implementation on this box's host cores."""
     if rank != 0:
@@ -186,8 +193,8 @@ def run_reference(args, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "plain PBILS: ER(1000, 0.5, graph seed 1), k=5, pop=128, gww=0.1",
-                       "sample": f"{sample_iters} iterations per step (of 100)", "early_stop": 100},
+            "config": {"workload": workload_text("plain", cfg),
+                       "sample": f"{sample_iters} iterations per step (of 100)", "parallelism": "replicas x1"},
             "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
                              "sample": f"{sample_iters} of the 100 iterations, --threads 0"},
             "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -581,9 +588,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32" if n > 32767 else "int16",
             "data": "synthetic",
-            "config": {"workload": f"{args.workload} PBILS: ER(n={n}, p={cfg['density']}, graph seed "
-                                   f"{cfg['graph_seed']}), k={k}, pop={pop}, tournament 5, perturb 0.4, gww 0.1, "
-                                   f"{cfg['iterations']} iterations (early stop off), seed {cfg['seed']} + rank",
+            "config": {"workload": workload_text(args.workload, cfg),
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                        "kernel_plan": solver.describe()},
             "ls_moves_per_s": moves_all / (total_ms_all * 1e-3),
