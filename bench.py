@@ -65,7 +65,9 @@ def parse():
     ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
     ap.add_argument("--serve-count", type=int, default=32, help="serving workload: requests")
     ap.add_argument("--serve-rate", type=float, default=10.0, help="serving workload: Poisson arrivals per second")
-    ap.add_argument("--serve-max-n", type=int, default=50000, help="serving workload: largest n")
+    ap.add_argument("--serve-max-n", type=int, default=32767,
+                    help="serving workload: largest n (the full stream goes to 50000; requests beyond 32767 run "
+                         "on side threads and take tens of seconds each, so the default sample stops there)")
     ap.add_argument("--serve-budget-gb", type=float, default=0.0, help="serving workload: HBM budget (0: 80%% free)")
     return ap.parse_args()
 
