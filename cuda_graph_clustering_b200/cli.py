@@ -17,13 +17,16 @@ import sys
 import numpy as np
 
 ALGORITHMS = ("pbils", "NeighborhoodCuda", "NeighborhoodWithManyLocalSearchesCuda")
+# the names the reference prints and writes (AlgorithmName, include/cc_cli.hpp:22-28)
+ALGORITHM_NAMES = {"pbils": "PBILS", "NeighborhoodCuda": "NeighborhoodCuda",
+                   "NeighborhoodWithManyLocalSearchesCuda": "NeighborhoodWithManyLocalSearchesCuda"}
 LS_KERNELS = {"auto": 0, "global": 1, "shared": 2, "wide": 3}
 
 
 def parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser(prog="cc_gpu", description="PBILS k-correlation clustering on the GPU")
     g = ap.add_argument_group("instance")
-    g.add_argument("--n", type=int, default=100, help="generate G(n, p) on N vertices")
+    g.add_argument("--n", type=int, default=500, help="generate G(n, p) on N vertices")
     g.add_argument("--density", type=float, default=0.5, help="edge probability")
     g.add_argument("--graph-seed", type=int, default=1, help="generator seed, fixes the instance")
     g.add_argument("--edges", default="", help="load an edge list (SNAP, CSV): any ids, a vertex is their rank")
@@ -113,7 +116,7 @@ def recount(graph, labels: np.ndarray, k: int) -> int:
 def write_result_json(path, graph, args, best, avg_objective, worst, avg_seconds):
     """WriteResultJson (include/cc_cli.hpp:248-277): the same keys in the same order."""
     lines = ["{",
-             f'  "algorithm": "{args.algorithm}",',
+             f'  "algorithm": "{ALGORITHM_NAMES[args.algorithm]}",',
              '  "backend": "gpu",',
              f'  "size": {graph.n},',
              f'  "edges": {graph.edges},',

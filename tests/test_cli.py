@@ -37,6 +37,7 @@ def test_parser_defaults_match_reference_params():
     a = parser().parse_args([])
     assert (a.k, a.pop, a.tournament, a.iters, a.early_stop, a.perturb, a.gww, a.seed) == \
         (2, 128, 5, 100, 6, 0.4, 0.1, 1)
+    assert (a.n, a.density, a.graph_seed, a.runs) == (500, 0.5, 1, 1)  # cli::Options (include/cc_cli.hpp:30-51)
     assert a.algorithm == "pbils" and a.ls_kernel == "auto" and a.verify
 
 
@@ -96,3 +97,33 @@ def test_drop_in_cc_gpu_solves_like_the_oracle(tmp_path, oracle, cuda_device):
     assert got["objective function value"] == want.objective
     assert got["clustering vector"] == [int(x) for x in want.labels]
     assert got["backend"] == "gpu"
+
+
+REF_CPU = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "cc_cpu")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CPU), reason="reference CPU binary not built")
+def test_result_json_matches_the_reference_writer(tmp_path):
+    """write_result_json emits the reference's WriteResultJson text: the same lines in the same order with the
+    same number formatting, except the backend name and the CPU-only threads line."""
+    import subprocess
+    from types import SimpleNamespace
+
+    import numpy as np
+
+    import cuda_graph_clustering_b200 as ccb
+    from cuda_graph_clustering_b200.cli import parser, write_result_json
+
+    ref_json = tmp_path / "ref.json"
+    flags = ["--n", "120", "--density", "0.3", "--graph-seed", "5", "--k", "3", "--pop", "8", "--iters", "4",
+             "--runs", "2"]
+    subprocess.run([REF_CPU, *flags, "--out", str(ref_json)], check=True, capture_output=True, timeout=120)
+    ref = json.loads(ref_json.read_text())
+    graph = ccb.Graph.ErdosRenyi(120, 0.3, 5)
+    best = SimpleNamespace(objective=ref["objective function value"], seconds=ref["computation time seconds"],
+                           clusters_used=ref["clusters used"], labels=np.array(ref["clustering vector"]))
+    ours = tmp_path / "ours.json"
+    write_result_json(str(ours), graph, parser().parse_args(flags), best, ref["objective average"],
+                      ref["objective max"], ref["computation time average"])
+    keep = lambda text: [l for l in text.splitlines() if '"backend"' not in l and '"threads"' not in l]
+    assert keep(ours.read_text()) == keep(ref_json.read_text())
