@@ -3,6 +3,10 @@
 Every comparison is exact: objective, labels (tie-breaking), iterations done, accepted moves, local
 searches and clusters used, as the reference's own GPU test compares them (cuda/cc_verify_gpu.cu:37-54).
 """
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -274,3 +278,21 @@ def test_one_call_cache_reuses_buffers_exactly(ccb, oracle, cuda_device):
     bits, edges = oracle.erdos_renyi(500, 0.3, 4)
     _same(ccb.SolveGpu(_graph(ccb, bits, edges), _params(ccb, **p)),
           oracle.pbils(bits, edges, make_params(**p)), "after release")
+
+
+_WIDE_GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                        "wide_reference.json")))
+
+
+@pytest.mark.parametrize("run", _WIDE_GOLDEN, ids=lambda r: f"n{r['n']}_k{r['k']}")
+def test_wide_matches_the_reference_binary_at_65536(ccb, cuda_device, run):
+    """At n = 65536 (the wide configuration's size) the GPU run equals the reference's own CPU solver
+    (tests/golden/make_wide_golden.py ran oracle/_ref/cc_cpu): objective, iterations, clusters used and the
+    labels' SHA-256."""
+    g = ccb.DeviceGraph.erdos_renyi(run["n"], run["density"], run["graph_seed"]).download()
+    got = ccb.SolveGpu(g, _params(ccb, k=run["k"], population=run["population"], iterations=run["iterations"],
+                                  seed=run["seed"]))
+    assert (got.objective, got.iterations_done, got.clusters_used) == \
+        (run["objective"], run["iterations_done"], run["clusters_used"])
+    labels = np.asarray(got.labels, dtype="<i4")
+    assert hashlib.sha256(labels.tobytes()).hexdigest() == run["labels_sha256"]
