@@ -1,11 +1,12 @@
 """Builds libccb.so in-tree for sm_100a (B200) with nvcc.
 
-    python -m cuda_graph_clustering_b200.build [--force] [--cc-gpu]
+    python -m cuda_graph_clustering_b200.build [--force] [--cc-gpu [REFERENCE_ROOT]]
 
 Every CUDA source is compiled with ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into an
 object under ``cuda_graph_clustering_b200/_build`` and linked into
 ``cuda_graph_clustering_b200/libccb.so``.  Objects are rebuilt only when a source or header is newer.
-With ``--cc-gpu`` it also links the drop-in ``cc_gpu`` binary (the reference's command line on libccb).
+With ``--cc-gpu`` it also links the drop-in ``cc_gpu`` binary (the reference's command line on libccb) from
+the reference checkout given after the flag or in CCB_REFERENCE.
 """
 from __future__ import annotations
 
@@ -72,15 +73,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-REFERENCE = os.environ.get("CCB_REFERENCE", "/root/reference")
 CC_GPU = os.path.join(PKG, "cc_gpu")
 
 
-def build_cc_gpu(reference: str = REFERENCE, verbose: bool = False) -> str | None:
+def build_cc_gpu(reference: str | None = None, verbose: bool = False) -> str | None:
     """The drop-in cc_gpu binary: the reference's own command line (include/cc_cli.hpp) and host sources
     (src/cc_graph.cpp, src/cc_pbils_cpu.cpp), compiled where they lie, linked with cc_gpu_ccb.cpp (the
-    reference's GPU entry points over libccb) and libccb.so.  Returns its path, or None without the reference
-    sources."""
+    reference's GPU entry points over libccb) and libccb.so.  `reference` is the reference checkout's root
+    (default: the CCB_REFERENCE environment variable).  Returns the binary's path, or None when no checkout
+    is given or it lacks those sources."""
+    reference = reference or os.environ.get("CCB_REFERENCE")
+    if not reference:
+        return None
     inc = os.path.join(reference, "include")
     srcs = [os.path.join(reference, "src", f) for f in ("cc_graph.cpp", "cc_pbils_cpu.cpp")]
     if not all(os.path.exists(x) for x in [inc] + srcs):
@@ -101,5 +105,6 @@ def build_cc_gpu(reference: str = REFERENCE, verbose: bool = False) -> str | Non
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
-    if "--cc-gpu" in sys.argv:
-        print(build_cc_gpu(verbose=True))
+    if "--cc-gpu" in sys.argv:  # python -m cuda_graph_clustering_b200.build --cc-gpu [REFERENCE_ROOT]
+        at = sys.argv.index("--cc-gpu")
+        print(build_cc_gpu(sys.argv[at + 1] if at + 1 < len(sys.argv) else None, verbose=True))

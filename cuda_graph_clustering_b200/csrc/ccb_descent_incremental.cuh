@@ -299,7 +299,7 @@ __device__ __forceinline__ void DescentIncremental(const DescentArgs<GainT>& a, 
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }
@@ -528,7 +528,7 @@ __device__ __forceinline__ void DescentIncrementalRegs(const DescentArgs<int16_t
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }

@@ -160,7 +160,7 @@ __device__ __forceinline__ void DescentRegisters(const DescentArgs<int16_t>& a, 
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }

@@ -187,7 +187,7 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }

@@ -191,7 +191,7 @@ __device__ __forceinline__ void DescentWidePacked(const DescentArgs<int32_t>& a,
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }
@@ -362,7 +362,7 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
     // neighbours of v: e += 2 (to = 1) or -= 2 (to = 0); the cluster whose best gets worse is 1 resp. 0
@@ -579,7 +579,7 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
     const Word step = (static_cast<Word>(1) << (20 * to)) - (static_cast<Word>(1) << (20 * from));

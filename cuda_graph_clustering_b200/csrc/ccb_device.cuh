@@ -24,10 +24,14 @@ struct Control {
   unsigned long long moves; // accepted local-search moves, summed over all descents
   unsigned long long t0_ns; // %globaltimer at solve start, for the device-side time limit
   int32_t record_slot;      // slot the record last came from
-  int32_t error;            // nonzero when a bounded device-side wait gave up
+  int32_t error;            // kErrorMoveBound or kErrorWaitTimeout (0: none)
   int32_t iter;             // current iteration of a batched instance (the plain path passes it as argument)
   int32_t pad;
 };
+
+// Values of Control::error.
+constexpr int32_t kErrorMoveBound = 1;    // a descent exceeded its move bound (inconsistent state)
+constexpr int32_t kErrorWaitTimeout = 2;  // a bounded wait on a kernel's own pipeline barriers gave up
 
 // One line of the --verbose progress log, written by the record kernel.
 struct TraceEntry {

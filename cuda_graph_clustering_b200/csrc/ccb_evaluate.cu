@@ -152,6 +152,12 @@ int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_
 // The array's host-side name is only a stand-in, not a device address, so the entry point looks the
 // address up with cudaGetSymbolAddress once per device (on its first call on that device, with that
 // device current) and passes it to the kernel.  Make that first call before any stream capture.
+// Under CUDA's default lazy module loading the array is only allocated when that first call loads this
+// module onto the device, so a caller that reserves the device's free memory for its own pool must make
+// the first call before it does; a call with count = 0 does exactly this set-up and nothing else.  (With
+// CUDA_MODULE_LOADING=EAGER the array is allocated when the library is loaded.)  The address is kept for
+// the life of the process: after cudaDeviceReset on a device the module is loaded afresh and may sit
+// elsewhere, so the entry point must not be used across a device reset.
 // Every call shares the one array and finds the last call's contents there.  k_evaluate writes every
 // mask word it later reads, so nothing needs clearing between calls; but two calls whose kernels
 // overlap on the GPU (different streams, or different host threads) race on the array, so callers
@@ -198,7 +204,6 @@ int ccb_evaluate_labelings_noalloc(const uint32_t* bits, uint32_t n, uint32_t wo
   if (const char* why = CheckEvaluateArgs(bits, n, words_per_row, k, count, labels, f_out)) {
     return Report(CCB_ERR_INVALID, why);
   }
-  if (count == 0) return Report(CCB_OK, "");
   const size_t words = (n + 31) / 32;
   if ((size_t)count * (size_t)k * words > kNoAllocMaskWords) {
     return Report(CCB_ERR_INVALID,
@@ -206,8 +211,9 @@ int ccb_evaluate_labelings_noalloc(const uint32_t* bits, uint32_t n, uint32_t wo
                   "its static scratch; split the batch or use ccb_evaluate_labelings");
   }
   uint32_t* masks = nullptr;
-  cudaError_t e = NoAllocScratch(&masks);
+  cudaError_t e = NoAllocScratch(&masks);  // also the whole of a count = 0 call: the per-device set-up
   if (e != cudaSuccess) return Report(CCB_ERR_CUDA, cudaGetErrorString(e));
+  if (count == 0) return Report(CCB_OK, "");
   k_evaluate<<<count, kEvalThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       bits, (int)n, (int)words, (int)words_per_row, (long long)edges, k, labels, masks, f_out, sizes_out, g_out);
   e = cudaGetLastError();

@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_descent(DescentArgs<GainT> a) {
     // Every accepted move lowers f by at least one and f >= 0, so f of the start state bounds the
     // number of moves; passing it means an inconsistent state, reported instead of looping on.
     if (static_cast<long long>(applied) > move_budget) {
-      if (tid == 0) atomicExch(&a.ctl->error, 1);
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
       break;
     }
   }

@@ -104,6 +104,15 @@ void CheckNeighborhood(const ccb_params& p, uint32_t n) {
   }
 }
 
+// The device's error flag (Control::error) after a solve: kErrorMoveBound from a descent that exceeded its move
+// bound, kErrorWaitTimeout from a kernel whose bounded wait on its own pipeline gave up.
+void CheckDeviceError(const Control& c) {
+  if (c.error == kErrorWaitTimeout) {
+    Fail(CCB_ERR_TIMEOUT, "a bounded device-side wait of the tensor-core rebuild gave up");
+  }
+  if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+}
+
 int CountClustersUsed(const int32_t* labels, uint32_t n, int k) {
   std::vector<char> seen(std::max(k, 1), 0);
   int used = 0;
@@ -471,6 +480,14 @@ struct ccb_solver {
 
 namespace {
 
+// The plan in words (ccb_solver_describe, --verbose); redone whenever the plan changes.
+void Describe(ccb_solver& s) {
+  char text[256];
+  std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory",
+                KernelName(s.plan), s.plan.threads, s.pop, s.plan.smem_bytes);
+  s.description = text;
+}
+
 ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   TraceRange trace_range("ccb.solver.create");
   std::unique_ptr<ccb_solver> s(new ccb_solver());
@@ -549,10 +566,7 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   } else {
     LaunchDescent<int16_t>(s->plan, DescentArgs<int16_t>{}, 0, nullptr, true);
   }
-  char text[256];
-  std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory",
-                KernelName(s->plan), s->plan.threads, pop, s->plan.smem_bytes);
-  s->description = text;
+  Describe(*s);
   return s.release();
 }
 
@@ -729,7 +743,7 @@ void RunPbils(ccb_solver& s, const ccb_params& p, cudaStream_t st, int32_t* labe
   }
   CopyOutLabels(s, labels_out, st);
   const Control& c = s.host_ctl[0];
-  if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+  CheckDeviceError(c);
   res->objective = c.record_f;
   res->iterations_done = c.iterations_done;
   res->local_searches = (int64_t)c.iterations_done * pop;
@@ -783,7 +797,7 @@ void RunNeighborhood(ccb_solver& s, const ccb_params& p, bool local_search, cuda
   }
   CopyOutLabels(s, labels_out, st);
   const Control& c = s.host_ctl[0];
-  if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+  CheckDeviceError(c);
   res->objective = c.record_f;
   res->iterations_done = 0;
   res->local_searches = local_search ? n : 0;
@@ -1233,7 +1247,7 @@ void RunBatch(ccb_batch& b) {
     ccb_solver& s = *in.solver;
     CopyOutLabels(s, in.labels.data(), st);
     const Control& c = s.host_ctl[0];
-    if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+    CheckDeviceError(c);
     in.result.objective = c.record_f;
     in.result.iterations_done = c.iterations_done;
     in.result.local_searches = (int64_t)c.iterations_done * s.pop;
@@ -1559,7 +1573,7 @@ void RetireLane(ccb_server& sv, ccb_server::Lane& L, std::vector<int>& finished)
     std::vector<int32_t> labels(s.n);
     CopyOutLabels(s, labels.data(), L.stream);
     const Control& c = s.host_ctl[0];
-    if (c.error) Fail(CCB_ERR_STATE, "descent exceeded its move bound: inconsistent device state");
+    CheckDeviceError(c);
     ccb_result r{};
     r.objective = c.record_f;
     r.iterations_done = c.iterations_done;
@@ -1959,6 +1973,7 @@ ccb_solver& CachedSolver(const uint32_t* bits, uint32_t n, uint32_t words_per_ro
     // the plan's k = 2 / 3 wide form depends on the density
     ccb_solver& s = *c.solver;
     s.plan.sparse = s.plan.packed_wide && 2.0 * (double)edges <= (double)n * n / 8.0;
+    Describe(s);
     return s;
   }
   c.Release();

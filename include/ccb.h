@@ -238,10 +238,13 @@ int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_
 /* No counterpart in the reference.  ccb_evaluate_labelings for callers that cannot allocate device
  * memory when they call in (their device memory is already reserved by their own pool allocator, or
  * their loop must not pay cudaMalloc/cudaFree and the device-wide synchronisation cudaFree can cause).
- * Allocates nothing: the mask scratch is a fixed 4 MiB array in device memory that every GPU loading
- * libccb.so holds until exit.  Limit: count * k * ceil(n / 32) <= 1048576 mask words, else
- * CCB_ERR_INVALID.  The first call on a device looks the array's device address up (make it before any
- * stream capture); all calls share the array, so calls whose kernels overlap on the GPU race and must
+ * Allocates nothing: the mask scratch is a fixed 4 MiB array in device memory that every GPU holds
+ * until exit once libccb.so's module is loaded on it.  Limit: count * k * ceil(n / 32) <= 1048576 mask
+ * words, else CCB_ERR_INVALID.  The first call on a device is its set-up: it looks the array's device
+ * address up and, under CUDA's default lazy module loading, is when the 4 MiB are taken.  Make it before
+ * any stream capture and before a pool of the caller's reserves the free memory; a call with count = 0
+ * does only this set-up.  The address is kept for the process: do not use this entry point across a
+ * cudaDeviceReset.  All calls share the array, so calls whose kernels overlap on the GPU race and must
  * be ordered by the caller.  Same arguments, outputs and asynchrony as ccb_evaluate_labelings. */
 int ccb_evaluate_labelings_noalloc(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                                    int32_t k, int32_t count, const int32_t* labels, int64_t* f_out,

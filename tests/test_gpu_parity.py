@@ -284,9 +284,10 @@ _WIDE_GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__fil
                                         "wide_reference.json")))
 
 
-@pytest.mark.parametrize("run", _WIDE_GOLDEN, ids=lambda r: f"n{r['n']}_k{r['k']}")
-def test_wide_matches_the_reference_binary_at_65536(ccb, cuda_device, run):
-    """At n = 65536 (the wide configuration's size) the GPU run equals the reference's own CPU solver
+@pytest.mark.parametrize("run", _WIDE_GOLDEN, ids=lambda r: f"n{r['n']}_k{r['k']}_p{r['density']}")
+def test_matches_the_reference_binary_at_large_sizes(ccb, cuda_device, run):
+    """At n = 65536 (the wide configuration's size, at p = 0.005 and at its own p = 0.02) and at n = 32000,
+    k = 8 (the narrow limit's large configuration) the GPU run equals the reference's own CPU solver
     (tests/golden/make_wide_golden.py ran oracle/_ref/cc_cpu): objective, iterations, clusters used and the
     labels' SHA-256."""
     g = ccb.DeviceGraph.erdos_renyi(run["n"], run["density"], run["graph_seed"]).download()

@@ -27,6 +27,8 @@ def _outputs(torch, count, k, n):
 
 def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(ccb, oracle, cuda_device):
     import torch
+    # a count = 0 call is the per-device set-up (symbol lookup, module load) and touches no pointer
+    ccb.evaluate_labelings_noalloc(0, 0, 0, 0, 2, 0, 0, 0)
     for n, k, count, gseed, lseed in [(1500, 9, 6, 3, 4), (700, 4, 11, 5, 6)]:
         bits, edges, dbits, dlab = _device_inputs(torch, oracle, n, k, count, gseed, lseed)
         f0, s0, g0 = _outputs(torch, count, k, n)
@@ -47,3 +49,25 @@ def test_noalloc_rejects_batches_beyond_its_scratch(ccb, oracle, cuda_device):
     with pytest.raises(RuntimeError) as e:
         ccb.evaluate_labelings_noalloc(f.data_ptr(), n, n // 32, 0, k, count, f.data_ptr(), f.data_ptr())
     assert "exceeds the 1048576 mask words" in str(e.value)
+
+
+def test_noalloc_full_scratch_without_optional_outputs(ccb, oracle, cuda_device):
+    """A batch that fills the scratch exactly (32 * 64 * 512 = 1048576 mask words, the last word included),
+    with sizes_out and g_out NULL, twice in a row: f equals the allocating entry point's."""
+    import torch
+    n, k, count = 16384, 64, 32
+    assert count * k * ((n + 31) // 32) == 1 << 20
+    for gseed, lseed in [(11, 12), (13, 14)]:
+        bits, edges = oracle.erdos_renyi(n, 0.03, gseed)
+        labels = np.random.default_rng(lseed).integers(0, k, (count, n)).astype(np.int32)
+        labels[-1, -32:] = k - 1  # the last labeling's last word: the array's final mask word is nonzero
+        dbits = torch.from_numpy(bits.view(np.int32)).cuda()
+        dlab = torch.from_numpy(labels).cuda()
+        f0 = torch.full((count,), -7, dtype=torch.int64, device="cuda")
+        f1 = torch.full((count,), -7, dtype=torch.int64, device="cuda")
+        ccb.evaluate_labelings_noalloc(dbits.data_ptr(), n, bits.shape[1], edges, k, count, dlab.data_ptr(),
+                                       f1.data_ptr())
+        ccb.evaluate_labelings(dbits.data_ptr(), n, bits.shape[1], edges, k, count, dlab.data_ptr(), f0.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(f0, f1)
+        assert int(f1[-1]) == oracle.objective_bitwise(bits, labels[-1])
