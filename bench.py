@@ -51,6 +51,9 @@ WIDE2 = dict(n=65536, density=0.02, graph_seed=1, k=2, population=128, tournamen
              iterations=50, early_stop=50, seed=1)
 WIDE3 = dict(WIDE2, k=3)
 WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "large": (LARGE, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {})}
+# The Neighborhood configuration: the planted two-community graph, n = 4096 split 2048/2048 by a seeded
+# permutation, p_in 0.6, p_out 0.1 (graph seed 1), batches of 128 start partitions (32 full batches).
+NEIGHBORHOOD = dict(n=4096, parts=2, shuffle_split=True, p_in=0.6, p_out=0.1, flip=0.0, graph_seed=1, batch=128)
 
 
 def parse():
@@ -59,7 +62,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="plain")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving", "neighborhood"],
+                    default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256, help="batched workload: instances")
     ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
@@ -441,6 +445,147 @@ def run_serving(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_neighborhood(args, rank, world, local):
+    """The Neighborhood configuration (NEIGHBORHOOD): one step = one NeighborhoodWithManyLocalSearchesCuda solve
+    (all 4096 start partitions, each followed by a local search) on the device-resident graph; the solve without
+    the local search (NeighborhoodCuda) is timed beside it.  Metric: accepted local-search moves per second.
+    Every step's objective, moves and labels must equal tests/golden/neighborhood_reference.json (the oracle's
+    and the reference's brute force, which agreed).  `e2e`: the one-call ABI from a pinned host bitset."""
+    import hashlib
+
+    import numpy as np
+    import torch
+
+    import cuda_graph_clustering_b200 as ccb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    c = NEIGHBORHOOD
+    golden = json.load(open(os.path.join(REPO, "tests", "golden", "neighborhood_reference.json")))
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    dg, _ = ccb.DeviceGraph.planted(c["n"], c["parts"], c["p_in"], c["p_out"], c["flip"], c["graph_seed"],
+                                    shuffle_split=c["shuffle_split"], stream=sh)
+    graph = dg.download()
+    params = ccb.PbilsParams(k=2, population=c["batch"])
+    solver = ccb.Solver(dg, params)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def exact(r, key):
+        w = golden[key]
+        return (r.objective == w["objective"] and r.accepted_moves == w["accepted_moves"]
+                and hashlib.sha256(np.asarray(r.labels, dtype="<i4").tobytes()).hexdigest() == w["labels_sha256"])
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        solver.neighborhood(params, True, stream=sh)
+        solver.neighborhood(params, False, stream=sh)
+    clocks = ClockSampler(local)
+    timed = {}
+    results = {}
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for ls in (True, False):
+        events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+        out = []
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                events[i][0].record(stream)
+            out.append(solver.neighborhood(params, ls, stream=sh))
+            events[i][1].record(stream)
+        torch.cuda.synchronize()
+        timed[ls] = sum(a.elapsed_time(b) for a, b in events)
+        results[ls] = out
+    barrier()
+    clock_info = clocks.stop()
+    bit_exact = all(exact(r, "local_search") for r in results[True]) and \
+        all(exact(r, "plain") for r in results[False])
+
+    solver.set_profiling(True)
+    prof = solver.neighborhood(params, True, stream=sh)
+    st = solver.stats()
+    solver.set_profiling(False)
+    descent_ms = st.descent_ms / max(st.descent_launches, 1)
+
+    pinned = torch.empty(graph.bits.size, dtype=torch.int32, pin_memory=True)
+    pinned.numpy().view(np.uint32)[:] = graph.bits.reshape(-1)
+    g_pinned = ccb.Graph(graph.n, pinned.numpy().view(np.uint32).reshape(graph.bits.shape), graph.edges)
+    ccb.SolveNeighborhoodWithManyLocalSearchesGpu(g_pinned, params)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_ok = True
+    for _ in range(args.steps):
+        e2e_ok &= exact(ccb.SolveNeighborhoodWithManyLocalSearchesGpu(g_pinned, params), "local_search")
+    e2e_s = time.perf_counter() - t0
+    moves = sum(r.accepted_moves for r in results[True])
+    (t_ls, t_plain, t_e2e), (moves_all,) = combine_over_ranks(dist, [timed[True], timed[False], e2e_s], [moves])
+
+    if rank == 0:
+        n = c["n"]
+        words = (n + 31) // 32
+        deg = 2.0 * graph.edges / n
+        moves_per_launch = prof.accepted_moves / max(st.descent_launches, 1)
+        per_move = n * (2 * 2 + 1) + 4 * words + 8 * deg  # SURVEY 8(d) generic move bytes at k = 2, sG = 2
+        modelled = moves_per_launch * per_move / (descent_ms * 1e-3) / 1e9
+        peak, peak_kind = measured_peak_hbm()
+        cpu = None
+        if not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(REPO, "oracle"))
+            from oracle import Reference
+            if Reference.available():
+                sample = 512
+                t1 = time.perf_counter()
+                _, ref_moves = Reference().neighborhood_range(graph.bits, True, 0, sample)
+                dt = time.perf_counter() - t1
+                cpu = {"value": ref_moves / dt, "unit": "moves/s", "cores": 1, "kind": "reference",
+                       "sample": f"start vertices 0..{sample - 1} of {n} with the local search (the reference's "
+                                 "sequential brute force, cuda/cc_verify_gpu.cu:21-35, on its own CPU State)",
+                       "neighborhoods_per_s": sample / dt}
+        line = {
+            "metric": "Neighborhood LS moves/s", "value": moves_all / (t_ls * 1e-3), "unit": "moves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ls / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "config": {"workload": f"Neighborhood k=2: planted n={n} split 2048/2048 (seeded permutation, graph seed "
+                                   f"{c['graph_seed']}), p_in {c['p_in']}, p_out {c['p_out']}, batch {c['batch']}, "
+                                   "NeighborhoodWithManyLocalSearchesCuda (all start vertices)",
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                       "kernel_plan": solver.describe()},
+            "neighborhoods_per_s": world * n * args.steps / (t_ls * 1e-3),
+            "plain_neighborhood_solves_per_s": world * args.steps / (t_plain * 1e-3),
+            "bit_exact": bool(bit_exact),
+            "objective": results[True][0].objective,
+            "e2e": {"value": moves_all / t_e2e, "unit": "moves/s", "h2d_bytes_per_step": int(graph.bits.nbytes),
+                    "d2h_bytes_per_step": int(4 * n + 48), "bit_exact": bool(e2e_ok)},
+            "roofline": {"bound": "alu", "kernel": "k_descent", "avg_launch_ms": descent_ms,
+                         "note": "state in registers and shared memory; see the plain workload's ALU-pipe profile",
+                         "modelled_bytes": {"achieved_gbs": modelled, "hbm_peak_gbs": peak, "peak_kind": peak_kind,
+                                            "frac": modelled / peak,
+                                            "per_move": "n(2k+1) + 4 ceil(n/32) + 8 deg (SURVEY 8(d))"}},
+            "kernel_ms_per_solve": {"descent": st.descent_ms, "rebuild": st.rebuild_ms, "record": st.record_ms,
+                                    "other": st.other_ms},
+            # per step pair: the solve with the local search, and the one without (no descent launches)
+            "gpu_launches": int(args.steps * (st.descent_launches + 2 * (st.rebuild_launches + st.record_launches
+                                                                         + st.other_launches))),
+            "clocks": clock_info,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -452,6 +597,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args, rank, world, local)
+        return
+    if args.workload == "neighborhood":
+        run_neighborhood(args, rank, world, local)
         return
 
     import numpy as np
@@ -576,10 +724,16 @@ def main():
         traffic = profiled_traffic(f"k_descent_{args.workload}")
         value = iters_all / (total_ms_all * 1e-3)
         cpu = None
-        if cfg["n"] > 32767:
-            cpu = {"value": None, "unit": "iter/s", "cores": None, "kind": "reference",
-                   "sample": "not run: one CPU iteration at this size takes minutes (17-52 G popcounts per rebuild)"}
-        elif not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu")):
+        have_ref = os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu"))
+        if cfg["n"] > 32767 and not args.no_cpu_baseline and have_ref:
+            # one iteration at population 8 (its time includes the initial rebuild of the 8 slots), scaled to
+            # the configuration's population 128: CPU time per iteration grows in proportion to the population
+            small = dict(cfg, population=8)
+            t, f, threads = reference_cpu_run(small, 1)
+            cpu = {"value": 8.0 / (cfg["population"] * t), "unit": "iter/s", "cores": threads, "kind": "reference",
+                   "sample": f"1 iteration at population 8 ({t:.1f} s, initial rebuild included), scaled by 8/128 "
+                             "to population 128; --threads 0"}
+        elif not args.no_cpu_baseline and have_ref:
             sample = 20 if args.workload == "plain" else 1
             t, f, threads = reference_cpu_run(cfg, sample)
             cpu = {"value": sample / t, "unit": "iter/s", "cores": threads, "kind": "reference",

@@ -215,6 +215,9 @@ class DeviceGraph:
             pass
 
 
+REBUILD_KINDS = {"auto": 0, "popcount": 1, "tensor": 2}
+
+
 class Solver:
     """Reusable buffers and kernel plan for (graph, k, population, ls_kernel) (ccb_solver_*)."""
 
@@ -228,6 +231,10 @@ class Solver:
 
     def describe(self) -> str:
         return lib().ccb_solver_describe(self.handle).decode()
+
+    def set_rebuild(self, kind: str) -> None:
+        """How G = A*Z is rebuilt (ccb_solver_set_rebuild): "auto", "popcount" or "tensor" (int8 tcgen05)."""
+        check(lib().ccb_solver_set_rebuild(self.handle, REBUILD_KINDS[kind]))
 
     def set_profiling(self, on: bool) -> None:
         check(lib().ccb_solver_set_profiling(self.handle, int(on)))
@@ -279,6 +286,14 @@ def evaluate_labelings_noalloc(bits_ptr: int, n: int, words_per_row: int, edges:
     its scratch is a fixed 4 MiB device array (count * k * ceil(n / 32) <= 1048576 mask words)."""
     check(lib().ccb_evaluate_labelings_noalloc(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr,
                                                sizes_ptr, g_ptr, stream or None))
+
+
+def evaluate_labelings_tensor(bits_ptr: int, n: int, words_per_row: int, edges: int, k: int, count: int,
+                              labels_ptr: int, f_ptr: int, sizes_ptr: int | None = None, g_ptr: int | None = None,
+                              stream: int = 0) -> None:
+    """ccb_evaluate_labelings_tensor: the recount with G = A*Z on the tensor cores (same outputs)."""
+    check(lib().ccb_evaluate_labelings_tensor(bits_ptr, n, words_per_row, edges, k, count, labels_ptr, f_ptr,
+                                              sizes_ptr, g_ptr, stream or None))
 
 
 TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")

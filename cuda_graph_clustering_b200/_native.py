@@ -71,6 +71,7 @@ SIGNATURES = {
     "ccb_solver_describe": (C.c_char_p, [_vp]),
     "ccb_solver_destroy": (None, [_vp]),
     "ccb_solver_set_profiling": (C.c_int, [_vp, C.c_int32]),
+    "ccb_solver_set_rebuild": (C.c_int, [_vp, C.c_int32]),
     "ccb_solver_stats": (C.c_int, [_vp, C.POINTER(CcbKernelStats)]),
     "ccb_graph_generate_erdos_renyi": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _vp, C.POINTER(_vp)]),
     "ccb_graph_generate_planted": (C.c_int, [C.c_uint32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
@@ -99,6 +100,8 @@ SIGNATURES = {
                                          _vp, _vp, _vp]),
     "ccb_evaluate_labelings_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32,
                                                  _vp, _vp, _vp, _vp, _vp]),
+    "ccb_evaluate_labelings_tensor": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32,
+                                                _vp, _vp, _vp, _vp, _vp]),
     "ccb_generate_erdos_renyi": (C.c_uint64, [_vp, ]),  # argtypes set below (mixed scalar types)
     "ccb_generate_planted": (C.c_uint64, []),
 }

@@ -42,6 +42,169 @@ __device__ __forceinline__ void LanesMinMax(const int* x, int& lo, int& hi) {
   }
 }
 
+// ---- compact keys (n <= 1023) ---------------------------------------------------------------------------
+// With B = bit width of n <= 10 and S = B + 8, a vertex's lanes are
+//     foreign c:  L_c = (h_c << S) + c          own a:  L_a = ((h_a + P) << S) - 16 a,    P = 2^(B+1)
+// (|h| <= n < 2^B, so every foreign lane is below 2^(B+S) and the own lane above it: max = own, min = the best
+// foreign target, smaller cluster first).  Then the block's move key of the vertex is a single add:
+//     kmin - kmax + ((P + 1 + 2^B) << S) + (u << 8) = ((gain + 2^B) << S) | (u << 8) | (a << 4) | to,
+// gain + 2^B in [2, 2^(B+1)) since the gain is in [1 - n, n - 1]: smaller gain, then smaller vertex, as the
+// reference orders moves, with both clusters riding in the low byte.  A move (v: from -> to) changes lanes
+// `from` and `to` of every vertex by -/+ 2^S (sign by adjacency to v); the block dispatches once per move on
+// (from, to) to a scan that touches only those two lanes.  Keys are unsigned so that the lanes of absent
+// vertices (u >= n, ignored) wrap instead of overflowing.
+constexpr int kCompactMaxBits = 10;
+
+template <int K, int V, int kFrom, int kTo>
+__device__ __forceinline__ uint32_t CompactScan(uint32_t (&key)[V][K], const uint32_t (&rw)[V], uint32_t lane_bit,
+                                                const uint32_t (&cu)[V], unsigned valid, uint32_t step) {
+  uint32_t best = ~0u;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    if constexpr (kFrom >= 0) {
+      const uint32_t d = (rw[j] & lane_bit) ? step : 0u - step;
+      key[j][kFrom] += d;
+      key[j][kTo] -= d;
+    }
+    int lanes[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) lanes[c] = static_cast<int>(key[j][c]);
+    int kmin, kmax;
+    LanesMinMax<K>(lanes, kmin, kmax);
+    const uint32_t mk = static_cast<uint32_t>(kmin - kmax) + cu[j];
+    best = min(best, ((valid >> j) & 1) ? mk : ~0u);
+  }
+  return best;
+}
+
+// The scan of the move (from, to) with both lanes known at compile time: one uniform jump per move.
+template <int K, int V>
+__device__ __forceinline__ uint32_t CompactScanMove(int from, int to, uint32_t (&key)[V][K], const uint32_t (&rw)[V],
+                                                    uint32_t lane_bit, const uint32_t (&cu)[V], unsigned valid,
+                                                    uint32_t step) {
+#define CCB_COMPACT_TO(F, T)                                                 \
+  case T:                                                                    \
+    if constexpr ((F) < K && (T) < K && (F) != (T)) {                        \
+      return CompactScan<K, V, F, T>(key, rw, lane_bit, cu, valid, step);    \
+    }                                                                        \
+    break;
+#define CCB_COMPACT_FROM(F)                                                                                    \
+  case F:                                                                                                      \
+    switch (to) {                                                                                              \
+      CCB_COMPACT_TO(F, 0) CCB_COMPACT_TO(F, 1) CCB_COMPACT_TO(F, 2) CCB_COMPACT_TO(F, 3)                      \
+      CCB_COMPACT_TO(F, 4) CCB_COMPACT_TO(F, 5) CCB_COMPACT_TO(F, 6) CCB_COMPACT_TO(F, 7)                      \
+    }                                                                                                          \
+    break;
+  switch (from) {
+    CCB_COMPACT_FROM(0) CCB_COMPACT_FROM(1) CCB_COMPACT_FROM(2) CCB_COMPACT_FROM(3)
+    CCB_COMPACT_FROM(4) CCB_COMPACT_FROM(5) CCB_COMPACT_FROM(6) CCB_COMPACT_FROM(7)
+  }
+#undef CCB_COMPACT_FROM
+#undef CCB_COMPACT_TO
+  return ~0u;  // not reached: from != to, both < K
+}
+
+template <int K, int T, int V>
+__device__ __forceinline__ void DescentRegistersCompact(const DescentArgs<int16_t>& a, int slot, int w,
+                                                        const uint32_t* rows, MoveRecord<uint32_t>* s_records) {
+  constexpr int kWarps = T / kWarp;
+  const int tid = threadIdx.x;
+  const int lane = tid % kWarp;
+  const int n = a.gr.n;
+  const int ld = a.ld;
+  const int bits = a.key_bits;
+  const int shift = bits + 8;
+  const uint32_t step = 1u << shift;
+  const uint32_t penalty = (2u << bits) << shift;
+
+  uint32_t key[V][K];
+  uint32_t cu[V];
+  unsigned valid = 0;
+  {
+    const int16_t* g_src = a.cur.g + static_cast<size_t>(w) * K * ld;
+    const uint8_t* l_src = a.cur.labels + static_cast<size_t>(w) * ld;
+    const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
+    int sz[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) sz[c] = sizes[c];
+    const uint32_t base = ((2u << bits) + 1u + (1u << bits)) << shift;
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int u = tid + j * T;
+      const bool ok = u < n;
+      valid |= ok ? (1u << j) : 0u;
+      const int own = ok ? l_src[u] : 0;
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        const int h = sz[c] - 2 * (ok ? static_cast<int>(g_src[static_cast<size_t>(c) * ld + u]) : 0);
+        const uint32_t lane_key = (static_cast<uint32_t>(h) << shift) + static_cast<uint32_t>(c);
+        key[j][c] = c == own ? lane_key + penalty - 17u * static_cast<uint32_t>(c) : lane_key;
+      }
+      cu[j] = base + (static_cast<uint32_t>(ok ? u : 0) << 8);
+    }
+  }
+  long long objective = a.cur.f[w];
+  const long long move_budget = objective;
+  unsigned long long applied = 0;
+  int parity = 0;
+  const uint32_t lane_bit = 1u << lane;
+  const uint32_t no_move = (1u << bits) << shift;
+  const uint32_t vmask = (1u << bits) - 1u;
+
+  uint32_t rw[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) rw[j] = 0u;
+  uint32_t best = CompactScan<K, V, -1, -1>(key, rw, lane_bit, cu, valid, step);
+  while (true) {
+    const uint32_t mkey = BlockArgMin<uint32_t, kWarps>(best, 0u, s_records + parity * kWarps).key;
+    if (mkey >= no_move) break;
+    parity ^= 1;
+    const int v = static_cast<int>((mkey >> 8) & vmask);
+    const int from = static_cast<int>((mkey >> 4) & 15u);
+    const int to = static_cast<int>(mkey & 15u);
+    if ((v % T) == tid) {  // the moved vertex's own lane moves from `from` to `to`
+      const int jv = v / T;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        if (j == jv) {
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            if (c == from) key[j][c] += 17u * static_cast<uint32_t>(c) - penalty;
+            if (c == to) key[j][c] += penalty - 17u * static_cast<uint32_t>(c);
+          }
+        }
+      }
+    }
+    objective += static_cast<long long>(static_cast<int>(mkey >> shift) - (1 << bits));
+    ++applied;
+    if (static_cast<long long>(applied) > move_budget) {
+      if (tid == 0) atomicExch(&a.ctl->error, kErrorMoveBound);
+      break;
+    }
+    const uint32_t* row = rows + static_cast<size_t>(v) * a.gr.pitch;
+#pragma unroll
+    for (int j = 0; j < V; ++j) rw[j] = ((valid >> j) & 1) ? row[(tid + j * T) >> 5] : 0u;  // words < ceil(n/32)
+    best = CompactScanMove<K, V>(from, to, key, rw, lane_bit, cu, valid, step);
+  }
+
+  uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    if ((valid >> j) & 1) {
+      int lanes[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) lanes[c] = static_cast<int>(key[j][c]);
+      int kmin, kmax;
+      LanesMinMax<K>(lanes, kmin, kmax);
+      dst[tid + j * T] = static_cast<uint8_t>(((0u - static_cast<uint32_t>(kmax)) >> 4) & 15u);
+    }
+  }
+  if (tid == 0) {
+    a.next.f[slot] = objective;
+    if (applied) atomicAdd(&a.ctl->moves, applied);
+  }
+}
+
 template <int K, int T, int V, bool kSmemRows>
 __device__ __forceinline__ void DescentRegisters(const DescentArgs<int16_t>& a, int slot) {
   constexpr int kWarps = T / kWarp;
@@ -76,6 +239,12 @@ __device__ __forceinline__ void DescentRegisters(const DescentArgs<int16_t>& a, 
   __syncthreads();
   if (s_stop) return;
   const int w = s_winner;
+  if constexpr (T * V <= 1024) {
+    if (a.key_bits <= kCompactMaxBits) {
+      DescentRegistersCompact<K, T, V>(a, slot, w, rows, s_records);
+      return;
+    }
+  }
 
   int key[V][K];
   int ucode[V];  // (2^B << B) | u: adding gain << B gives the block-wide move key

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -32,6 +33,7 @@
 #include "ccb_util.h"
 #include "ccb_kernels.cuh"
 #include "ccb_plans.h"
+#include "ccb_rebuild_tensor.h"
 
 namespace ccb {
 
@@ -435,6 +437,8 @@ struct ccb_solver {
   int64_t* next_f = nullptr;
   uint32_t* masks = nullptr;
   int64_t* intra = nullptr;    // tiled rebuild (wide path): per-slot intra-cluster sums; null: per-slot rebuild
+  int rebuild_kind = CCB_REBUILD_AUTO;
+  std::unique_ptr<TensorRebuild> tensor;  // set: the wide path rebuilds G on the tensor cores
   int32_t* src_map = nullptr;
   int32_t* order = nullptr;
   uint8_t* record_lab = nullptr;
@@ -482,10 +486,50 @@ namespace {
 
 // The plan in words (ccb_solver_describe, --verbose); redone whenever the plan changes.
 void Describe(ccb_solver& s) {
-  char text[256];
-  std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory",
-                KernelName(s.plan), s.plan.threads, s.pop, s.plan.smem_bytes);
+  char text[320];
+  std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory%s",
+                KernelName(s.plan), s.plan.threads, s.pop, s.plan.smem_bytes,
+                s.tensor ? "; G rebuilt on the tensor cores (int8 tcgen05, TMA)" : "");
   s.description = text;
+}
+
+// CCB_REBUILD_AUTO's choice on the wide path.
+constexpr bool kTensorRebuildByDefault = false;
+
+// Whether the solver rebuilds G on the tensor cores: the tiled wide rebuild (int32 G) with n >= 128, chosen
+// explicitly or by CCB_REBUILD_AUTO.
+bool WantTensor(const ccb_solver& s, int kind) {
+  if (s.intra == nullptr || kind == CCB_REBUILD_POPCOUNT) return false;
+  if (kind == CCB_REBUILD_AUTO && !kTensorRebuildByDefault) return false;
+  TensorRebuild t;
+  const char* why = nullptr;
+  return PlanTensorRebuild(t, s.n, s.pop * s.k, &why);
+}
+
+// Sets the rebuild kind; allocates the one-hot buffer and encodes the tensor maps when the tensor path is on.
+void SetRebuild(ccb_solver& s, int kind) {
+  if (kind != CCB_REBUILD_AUTO && kind != CCB_REBUILD_POPCOUNT && kind != CCB_REBUILD_TENSOR) {
+    Fail(CCB_ERR_INVALID, "rebuild kind must be CCB_REBUILD_AUTO, CCB_REBUILD_POPCOUNT or CCB_REBUILD_TENSOR");
+  }
+  if (kind == CCB_REBUILD_TENSOR && !WantTensor(s, kind)) {
+    Fail(CCB_ERR_INVALID, "the tensor-core rebuild runs on the wide path (int32 G: n > 32767 or --ls-kernel wide) "
+                          "with n >= 128");
+  }
+  s.rebuild_kind = kind;
+  if (!WantTensor(s, kind)) {
+    s.tensor.reset();
+    return;
+  }
+  if (s.tensor) return;
+  std::unique_ptr<TensorRebuild> t(new TensorRebuild());
+  const char* why = nullptr;
+  PlanTensorRebuild(*t, s.n, s.pop * s.k, &why);
+  uint8_t* z = nullptr;
+  s.Alloc(z, (size_t)t->z_rows * t->kz);
+  CCB_CUDA(cudaMemset(z, 0, (size_t)t->z_rows * t->kz));
+  CCB_CUDA(EncodeTensorRebuild(*t, s.graph->bits, s.graph->pitch, z));
+  s.device_bytes += (size_t)t->z_rows * t->kz;
+  s.tensor = std::move(t);
 }
 
 ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
@@ -566,6 +610,7 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   } else {
     LaunchDescent<int16_t>(s->plan, DescentArgs<int16_t>{}, 0, nullptr, true);
   }
+  SetRebuild(*s, CCB_REBUILD_AUTO);
   Describe(*s);
   return s.release();
 }
@@ -595,6 +640,27 @@ void LaunchRebuild(ccb_solver& s, int grid, int mode, const int32_t* src_map, ui
       const RebuildTilesArgs t{g.View(), s.cur_lab, s.masks, s.Cur<int32_t>().g, s.intra, grid, s.k, s.ld, mode, ctl};
       const int tiles = (g.n + kRebuildTileThreads / kWarp - 1) / (kRebuildTileThreads / kWarp);
       const size_t smem = (size_t)kRebuildTileThreads / kWarp * g.pitch * 4;
+      if (s.tensor) {
+        // labels, masks and sizes as above; then Z, the tensor-core contraction and f
+        const Control* stop = (mode == kRebuildPerturb || mode == kRebuildCopy) ? ctl : nullptr;
+        int32_t* error = reinterpret_cast<int32_t*>(reinterpret_cast<char*>(s.ctl) + offsetof(Control, error));
+        cudaError_t e = cudaSuccess;
+        s.timer.Time(kCatRebuild, st, [&] {
+          k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(a);
+          e = LaunchBuildZ<uint8_t>(*s.tensor, s.cur_lab, s.ld, grid, s.k, nullptr, 0, nullptr, nullptr, stop, st);
+          if (e == cudaSuccess) {
+            e = LaunchTensorRebuild<uint8_t>(*s.tensor, s.Cur<int32_t>().g, s.ld, g.n, grid, s.k, s.cur_lab, s.ld,
+                                             s.intra, error, stop, st);
+          }
+          if (e == cudaSuccess) {
+            k_rebuild_finish<GainT><<<(grid + 127) / 128, 128, 0, st>>>(s.Cur<GainT>(), s.intra, grid, s.k, s.kpad,
+                                                                        (int64_t)g.edges, mode, ctl);
+          }
+        });
+        CCB_CUDA(e);
+        CCB_CUDA(cudaGetLastError());
+        return;
+      }
       s.timer.Time(kCatRebuild, st, [&] {
         k_rebuild<GainT, kRebuildThreads><<<grid, kRebuildThreads, 0, st>>>(a);
         k_rebuild_tiles<kRebuildTileThreads><<<tiles, kRebuildTileThreads, smem, st>>>(t);
@@ -1739,6 +1805,14 @@ int ccb_solver_neighborhood(ccb_solver* s, const ccb_params* params, int32_t loc
     } else {
       RunNeighborhood<int16_t>(*s, *params, local_search != 0, st, labels_out, result);
     }
+  });
+}
+
+int ccb_solver_set_rebuild(ccb_solver* s, int32_t kind) {
+  return Guard([&] {
+    if (!s) Fail(CCB_ERR_STATE, "null solver");
+    SetRebuild(*s, kind);
+    Describe(*s);
   });
 }
 

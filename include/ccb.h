@@ -29,7 +29,7 @@ enum ccb_status {
   CCB_ERR_INVALID = 1,       /* parameters rejected (bad k, population, gww, n, ...) */
   CCB_ERR_DEVICE_MEMORY = 2, /* the run does not fit the free device memory / shared memory */
   CCB_ERR_CUDA = 3,          /* a CUDA runtime call failed */
-  CCB_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (batched / serving paths) */
+  CCB_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (the tensor-core rebuild's pipeline) */
   CCB_ERR_STATE = 5,         /* handle misuse (null handle, queue full, ...) */
   CCB_ERR_CANCELLED = 6      /* a served request was cancelled (ccb_server_cancel) */
 };
@@ -130,6 +130,14 @@ int ccb_solver_pbils(ccb_solver* solver, const ccb_params* params, void* stream,
 /* Neighborhood enumerators on the solver's graph (k must be 2). */
 int ccb_solver_neighborhood(ccb_solver* solver, const ccb_params* params, int32_t local_search, void* stream,
                             int32_t* labels_out, ccb_result* result);
+/* How a solver rebuilds G = A*Z after each perturbation.  No counterpart in the reference, whose rebuild is the
+ * popcount of cuda/cc_population_kernels.cuh:44-136 (KernelRebuild / KernelRebuild2).  CCB_REBUILD_TENSOR runs
+ * the whole population's rebuild as one int8 contraction on the tensor cores (tcgen05 kind::i8, int32
+ * accumulators in TMEM, operands fed by TMA): G[slot][c][v] = sum_u A[v][u] Z[slot*k + c][u] with Z the one-hot
+ * labels.  The counts are the same integers either way, so every trajectory is unchanged.  It applies to the
+ * wide path (int32 G: n > 32767, or ls_kernel CCB_LS_WIDE) with n >= 128; CCB_REBUILD_AUTO takes it there. */
+enum ccb_rebuild_kind { CCB_REBUILD_AUTO = 0, CCB_REBUILD_POPCOUNT = 1, CCB_REBUILD_TENSOR = 2 };
+int ccb_solver_set_rebuild(ccb_solver* solver, int32_t kind);
 /* Text description of the plan ("generic, shared memory, 512 threads, ..."). */
 const char* ccb_solver_describe(const ccb_solver* solver);
 void ccb_solver_destroy(ccb_solver* solver);
@@ -249,6 +257,15 @@ int ccb_evaluate_labelings(const uint32_t* bits, uint32_t n, uint32_t words_per_
 int ccb_evaluate_labelings_noalloc(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
                                    int32_t k, int32_t count, const int32_t* labels, int64_t* f_out,
                                    int32_t* sizes_out, int32_t* g_out, void* stream);
+
+/* No counterpart in the reference.  ccb_evaluate_labelings with G = A*Z computed on the tensor cores (the
+ * contraction of ccb_solver_set_rebuild's CCB_REBUILD_TENSOR): the same outputs, exactly.  Needs n >= 128,
+ * words_per_row a multiple of 4 and a 16-byte aligned bitset (its rows are read by TMA).  Scratch (the one-hot
+ * Z, count * k rows of ceil(ceil(n/32)/4) * 128 bytes) comes from the stream-ordered allocator.  A labeling's
+ * f is -2 if the kernel's bounded pipeline wait gave up.  Asynchronous on `stream`. */
+int ccb_evaluate_labelings_tensor(const uint32_t* bits, uint32_t n, uint32_t words_per_row, uint64_t edges,
+                                  int32_t k, int32_t count, const int32_t* labels, int64_t* f_out,
+                                  int32_t* sizes_out, int32_t* g_out, void* stream);
 
 /* ---- host instance generators (the instances of the reference's CLI and of the benchmarks) ----- */
 

@@ -192,6 +192,8 @@ class Reference:
         lib.ref_local_search.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, _i32p, _i64p]
         lib.ref_neighborhood.restype = C.c_int
         lib.ref_neighborhood.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, _i32p, C.POINTER(Result)]
+        lib.ref_neighborhood_range.restype = C.c_int64
+        lib.ref_neighborhood_range.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32, _i64p]
         lib.ref_objective_direct.restype = C.c_int64
         lib.ref_objective_direct.argtypes = [_u32p, C.c_uint32, C.c_uint32, _i32p]
         lib.ref_objective_bitwise.restype = C.c_int64
@@ -235,6 +237,13 @@ class Reference:
         self.lib.ref_neighborhood(np.ascontiguousarray(bits, np.uint32).reshape(-1), n, bits.shape[1],
                                   int(local_search), labels, C.byref(res))
         return Solution(res.objective, labels[:n], 0, res.clusters_used, res.local_searches, res.accepted_moves)
+
+    def neighborhood_range(self, bits, local_search: bool, first: int, count: int):
+        """The brute force over start vertices [first, first + count) only: (best f, accepted moves)."""
+        best = np.zeros(1, np.int64)
+        moves = self.lib.ref_neighborhood_range(np.ascontiguousarray(bits, np.uint32).reshape(-1), bits.shape[0],
+                                                bits.shape[1], int(local_search), first, count, best)
+        return int(best[0]), int(moves)
 
     def rebuild(self, bits, k, labels):
         n = bits.shape[0]

@@ -128,6 +128,25 @@ int ref_neighborhood(const uint32_t* bits, uint32_t n, uint32_t words, int local
   return 0;
 }
 
+// The same loop over start vertices [first, first + count) only: a bounded sample of the brute force, for
+// timing the reference's CPU Neighborhood on the GPU box (bench.py's CPU baseline).  Returns the moves.
+int64_t ref_neighborhood_range(const uint32_t* bits, uint32_t n, uint32_t words, int local_search, uint32_t first,
+                               uint32_t count, int64_t* best_out) {
+  const cc::Graph g = FromBits(bits, n, words);
+  cc::State s;
+  s.Init((int)n, 2);
+  long long best = -1;
+  long long moves = 0;
+  for (uint32_t v = first; v < first + count && v < n; ++v) {
+    for (uint32_t u = 0; u < n; ++u) s.labels[u] = (u == v || g.IsJoined(v, u)) ? 0 : 1;
+    s.Rebuild(g);
+    if (local_search) cc::LocalSearch(g, s, &moves);
+    if (best < 0 || s.f < best) best = s.f;
+  }
+  *best_out = best;
+  return moves;
+}
+
 int64_t ref_objective_direct(const uint32_t* bits, uint32_t n, uint32_t words, const int32_t* labels) {
   const cc::Graph g = FromBits(bits, n, words);
   return cc::ObjectiveDirect(g, std::vector<int>(labels, labels + n));
