@@ -50,7 +50,12 @@ LARGE = dict(n=32000, density=0.33, graph_seed=7, k=8, population=128, tournamen
 WIDE2 = dict(n=65536, density=0.02, graph_seed=1, k=2, population=128, tournament=5, perturbation=0.4, gww=0.1,
              iterations=50, early_stop=50, seed=1)
 WIDE3 = dict(WIDE2, k=3)
-WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "large": (LARGE, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {})}
+# The published docs/data/gpu.csv row at the narrow limit (line 26): ER(32000, 0.33, graph seed 7), k=3, pop 128,
+# 20 iterations, gww 0, early stop off, seed 6 -> f = 224579124 (GPU and CPU alike).
+GPUCSV32K = dict(n=32000, density=0.33, graph_seed=7, k=3, population=128, tournament=5, perturbation=0.4, gww=0.0,
+                 iterations=20, early_stop=1000, seed=6)
+WORKLOADS = {"plain": (PLAIN, PLAIN_OBJECTIVE), "large": (LARGE, {}), "wide2": (WIDE2, {}), "wide3": (WIDE3, {}),
+             "gpucsv32k": (GPUCSV32K, {6: 224579124})}
 # The Neighborhood configuration: the planted two-community graph, n = 4096 split 2048/2048 by a seeded
 # permutation, p_in 0.6, p_out 0.1 (graph seed 1), batches of 128 start partitions (32 full batches).
 NEIGHBORHOOD = dict(n=4096, parts=2, shuffle_split=True, p_in=0.6, p_out=0.1, flip=0.0, graph_seed=1, batch=128)
@@ -169,6 +174,24 @@ def reference_cpu_run(cfg, iterations, threads=0):
     f = int(re.search(r"objective\s+min=(\d+)", out).group(1))
     threads_used = int(re.search(r"threads\s+(\d+)", out).group(1))
     return t, f, threads_used
+
+
+def reference_gpu_run(cfg, runs=3):
+    """The reference's own GPU binary (oracle/_ref/cc_gpu_ref: its CUDA sources compiled for sm_100a) on the same
+    instance: (best solver seconds over `runs` runs of seeds seed .. seed + runs - 1, objective of the run with
+    this seed), or None when it was not built.  The first run also pays the CUDA context set-up."""
+    exe = os.path.join(REPO, "oracle", "_ref", "cc_gpu_ref")
+    if not os.path.exists(exe):
+        return None
+    cmd = [exe, "--n", str(cfg["n"]), "--density", str(cfg["density"]), "--graph-seed", str(cfg["graph_seed"]),
+           "--k", str(cfg["k"]), "--pop", str(cfg["population"]), "--tournament", str(cfg["tournament"]),
+           "--perturb", str(cfg["perturbation"]), "--gww", str(cfg["gww"]), "--iters", str(cfg["iterations"]),
+           "--early-stop", str(cfg["early_stop"]), "--seed", str(cfg["seed"]), "--runs", str(runs), "--no-verify"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True).stdout
+    # run r uses seed + r and the same fixed iteration count; run 0 has this instance's seed
+    t = float(re.search(r"time\s+best=([0-9.]+)s", out).group(1))
+    f = int(re.search(r"run 0\s+f=(\d+)", out).group(1))
+    return t, f
 
 
 def workload_text(name, cfg):
@@ -739,6 +762,17 @@ def main():
             cpu = {"value": sample / t, "unit": "iter/s", "cores": threads, "kind": "reference",
                    "sample": f"{sample} of the {cfg['iterations']} iterations of the same instance and seed, "
                              "--threads 0"}
+        ref_gpu = None
+        if args.workload in ("plain", "gpucsv32k") and not args.no_cpu_baseline:
+            got = reference_gpu_run(dict(cfg, seed=seed))
+            if got is not None:
+                t_ref, f_ref = got
+                ref_gpu = {"value": cfg["iterations"] / t_ref, "unit": "iter/s", "objective": f_ref,
+                           "same_objective": f_ref == results[0].objective,
+                           "binary": "oracle/_ref/cc_gpu_ref: the reference's cuda/ sources built for sm_100a",
+                           "timing": "its own solver time (PbilsResult.seconds, best of 3 runs; includes its "
+                                     "per-call allocation and bitset upload)",
+                           "ours_over_reference": value / (cfg["iterations"] / t_ref)}
         line = {
             "metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
@@ -763,6 +797,7 @@ def main():
             "gpu_launches": int(launches_per_solve * args.steps),
             "clocks": clock_info,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line))
     if dist is not None:
