@@ -197,6 +197,15 @@ class DeviceGraph:
                                                C.byref(h), comm.ctypes.data))
         return cls._wrap(h), comm[:n]
 
+    @classmethod
+    def load_tags(cls, path: str, similarity: str = "jaccard", threshold: float = 0.5, n: int = 0, seed: int = 1,
+                  stream: int = 0) -> "DeviceGraph":
+        """Graph::LoadTags (src/cc_graph.cpp:311-371) built on the device (ccb_graph_load_tags)."""
+        h = C.c_void_p()
+        check(lib().ccb_graph_load_tags(path.encode(), similarity.encode(), threshold, n, seed, stream or None,
+                                        C.byref(h)))
+        return cls._wrap(h)
+
     def download(self) -> Graph:
         w = words_per_row(self.n)
         bits = np.zeros((max(self.n, 1), w), np.uint32)

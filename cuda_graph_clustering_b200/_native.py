@@ -74,6 +74,8 @@ SIGNATURES = {
     "ccb_solver_set_rebuild": (C.c_int, [_vp, C.c_int32]),
     "ccb_solver_stats": (C.c_int, [_vp, C.POINTER(CcbKernelStats)]),
     "ccb_graph_generate_erdos_renyi": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _vp, C.POINTER(_vp)]),
+    "ccb_graph_load_tags": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_uint32, C.c_uint64, _vp,
+                                      C.POINTER(_vp)]),
     "ccb_graph_generate_planted": (C.c_int, [C.c_uint32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                              C.c_uint64, _vp, C.POINTER(_vp), _vp]),
     "ccb_graph_download": (C.c_int, [_vp, _vp, C.c_uint32]),

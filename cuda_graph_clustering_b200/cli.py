@@ -5,7 +5,8 @@ codes (include/cc_cli.hpp:124-183 flags, :284-377 Main, :248-277 WriteResultJson
 
 Instances: a seeded G(n, p) (``Graph::ErdosRenyi``, generated on the device bit-exactly) or an edge list
 (``--edges``: ``Graph::LoadEdgeList``, src/cc_graph.cpp:270-306 -- any integer ids, a vertex is the rank of its
-id, ``#`` / ``%`` comment lines and lines not starting with a number are skipped, self-loops dropped).  The
+id, ``#`` / ``%`` comment lines and lines not starting with a number are skipped, self-loops dropped) or a tags
+file (``--tags``: ``Graph::LoadTags``, src/cc_graph.cpp:311-371, built on the device).  The
 post-solve check recounts the objective on the GPU over the bit rows (``ccb_evaluate_labelings``, the
 reference's ``ObjectiveBitwise``); a mismatch exits 2, any error prints ``error: ...`` and exits 1.
 """
@@ -30,6 +31,10 @@ def parser() -> argparse.ArgumentParser:
     g.add_argument("--density", type=float, default=0.5, help="edge probability")
     g.add_argument("--graph-seed", type=int, default=1, help="generator seed, fixes the instance")
     g.add_argument("--edges", default="", help="load an edge list (SNAP, CSV): any ids, a vertex is their rank")
+    g.add_argument("--tags", default="", help="graph by tags ({\"key\": [\"tag\", ...]} JSON): n random objects "
+                                              "by --graph-seed, joined when --similarity >= --threshold")
+    g.add_argument("--similarity", default="jaccard", help="measure for --tags: jaccard, cosine, dice, overlap")
+    g.add_argument("--threshold", type=float, default=0.5, help="threshold for --tags")
     a = ap.add_argument_group("algorithm")
     a.add_argument("--algorithm", choices=ALGORITHMS, default="pbils")
     a.add_argument("--k", type=int, default=2, help="upper bound on the number of clusters")
@@ -142,7 +147,10 @@ def main(argv=None) -> int:
     import cuda_graph_clustering_b200 as ccb
 
     try:
-        if args.edges:
+        if args.tags:  # Graph::LoadTags (src/cc_graph.cpp:311-371), built on the device
+            graph = ccb.DeviceGraph.load_tags(args.tags, args.similarity, args.threshold, args.n,
+                                              args.graph_seed).download()
+        elif args.edges:
             graph = load_edge_list(args.edges)
         else:
             graph = ccb.DeviceGraph.erdos_renyi(args.n, args.density, args.graph_seed).download()

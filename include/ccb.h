@@ -115,6 +115,13 @@ int ccb_graph_generate_erdos_renyi(uint32_t n, double density, uint64_t seed, vo
  * community_out (host, n entries) may be NULL.  No counterpart in the reference. */
 int ccb_graph_generate_planted(uint32_t n, int32_t parts, int32_t shuffle_split, double p_in, double p_out,
                                double flip, uint64_t seed, void* stream, ccb_graph** out, int32_t* community_out);
+/* Graph::LoadTags (src/cc_graph.cpp:311-371) built on the device: the objects of a tags JSON file ({"key":
+ * ["tag", ...], ...}), n of them sampled by the seeded partial Fisher-Yates shuffle of SampleWithoutReplacement
+ * (all when n is 0 or at least their count), joined when the similarity of their tag sets ("jaccard", "cosine",
+ * "dice" or "overlap") is at least the threshold.  The same bits and edge count as the reference's loader;
+ * parse errors carry its messages. */
+int ccb_graph_load_tags(const char* path, const char* similarity, double threshold, uint32_t n, uint64_t seed,
+                        void* stream, ccb_graph** out);
 /* Copies a device graph back into the reference's host layout (n rows of words_per_row words). */
 int ccb_graph_download(const ccb_graph* graph, uint32_t* bits, uint32_t words_per_row);
 int ccb_graph_size(const ccb_graph* graph, uint32_t* n, uint64_t* edges);

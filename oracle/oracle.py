@@ -194,6 +194,9 @@ class Reference:
         lib.ref_neighborhood.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, _i32p, C.POINTER(Result)]
         lib.ref_neighborhood_range.restype = C.c_int64
         lib.ref_neighborhood_range.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32, _i64p]
+        lib.ref_load_tags.restype = C.c_int64
+        lib.ref_load_tags.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, _u32p,
+                                      C.POINTER(C.c_uint64)]
         lib.ref_objective_direct.restype = C.c_int64
         lib.ref_objective_direct.argtypes = [_u32p, C.c_uint32, C.c_uint32, _i32p]
         lib.ref_objective_bitwise.restype = C.c_int64
@@ -244,6 +247,17 @@ class Reference:
         moves = self.lib.ref_neighborhood_range(np.ascontiguousarray(bits, np.uint32).reshape(-1), bits.shape[0],
                                                 bits.shape[1], int(local_search), first, count, best)
         return int(best[0]), int(moves)
+
+    def load_tags(self, path: str, similarity: str, threshold: float, n: int, seed: int, capacity: int):
+        """The reference's own Graph::LoadTags: (bits [n][words_per_row], edges)."""
+        bits = np.zeros(max(1, capacity * words_per_row(capacity)), np.uint32)
+        edges = C.c_uint64()
+        size = self.lib.ref_load_tags(path.encode(), similarity.encode(), threshold, n, seed, capacity, bits,
+                                      C.byref(edges))
+        if size < 0:
+            raise RuntimeError("reference LoadTags failed")
+        size = int(size)
+        return bits[: size * words_per_row(size)].reshape(size, words_per_row(size)), int(edges.value)
 
     def rebuild(self, bits, k, labels):
         n = bits.shape[0]

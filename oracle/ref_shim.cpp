@@ -147,6 +147,21 @@ int64_t ref_neighborhood_range(const uint32_t* bits, uint32_t n, uint32_t words,
   return moves;
 }
 
+// Graph::LoadTags (src/cc_graph.cpp:311-371): writes up to `capacity` vertices' rows (max(1, ceil(n/32)) words
+// each) into bits and the edge count into edges_out; returns the vertex count, or -1 on an error.
+int64_t ref_load_tags(const char* path, const char* similarity, double threshold, uint32_t n, uint64_t seed,
+                      uint32_t capacity, uint32_t* bits, uint64_t* edges_out) {
+  try {
+    const cc::Graph g = cc::Graph::LoadTags(path, similarity, threshold, n, seed);
+    if (g.Size() > capacity) return -1;
+    std::memcpy(bits, g.Bits().data(), g.Bits().size() * sizeof(uint32_t));
+    *edges_out = g.EdgeCount();
+    return g.Size();
+  } catch (...) {
+    return -1;
+  }
+}
+
 int64_t ref_objective_direct(const uint32_t* bits, uint32_t n, uint32_t words, const int32_t* labels) {
   const cc::Graph g = FromBits(bits, n, words);
   return cc::ObjectiveDirect(g, std::vector<int>(labels, labels + n));
