@@ -344,18 +344,27 @@ def _ensure_tuning() -> None:
         load_tuning()
 
 
-class Batch:
-    """Many independent PBILS instances solved together (ccb_batch_*): one CUDA graph per iteration of all
-    instances, persistent per-bucket descent kernels fed by a device work queue.  Each result equals the
-    instance's plain solve bit for bit."""
+BATCH_ENGINES = {"flow": 0, "lockstep": 1}
 
-    def __init__(self):
+
+class Batch:
+    """Many independent PBILS instances solved together (ccb_batch_*) by persistent per-bucket kernels fed by
+    device work queues: the flow engine (default; every instance advances on its own) or the lock-step engine
+    (one CUDA graph replay per iteration of all instances).  Each result equals the instance's plain solve bit
+    for bit."""
+
+    def __init__(self, engine: str = "flow", wait_limit_sec: float = 0.0):
         _ensure_tuning()
         h = C.c_void_p()
         check(lib().ccb_batch_create(C.byref(h)))
         self.handle = h
         self.graphs = []
         self.sizes = []
+        check(lib().ccb_batch_set_engine(h, BATCH_ENGINES[engine], wait_limit_sec))
+
+    def withhold(self, i: int) -> None:
+        """Never publish instance i's work (host-side fault injection: the run ends in CCB_ERR_TIMEOUT)."""
+        check(lib().ccb_batch_withhold(self.handle, i))
 
     def add(self, graph: DeviceGraph, params: PbilsParams) -> int:
         p = params.to_c()

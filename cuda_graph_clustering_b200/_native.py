@@ -84,6 +84,8 @@ SIGNATURES = {
     "ccb_batch_run": (C.c_int, [_vp]),
     "ccb_batch_result": (C.c_int, [_vp, C.c_int32, _vp, C.POINTER(CcbResult)]),
     "ccb_batch_describe": (C.c_char_p, [_vp]),
+    "ccb_batch_set_engine": (C.c_int, [_vp, C.c_int32, C.c_double]),
+    "ccb_batch_withhold": (C.c_int, [_vp, C.c_int32]),
     "ccb_batch_destroy": (None, [_vp]),
     "ccb_release_cache": (None, []),
     "ccb_tuning_set": (C.c_int, [C.POINTER(CcbTuningEntry), C.c_int32]),

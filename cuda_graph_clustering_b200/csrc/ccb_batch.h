@@ -47,6 +47,34 @@ struct BatchShape {
 
 cudaError_t LaunchBatchDescent(const BatchShape& shape, const BatchEntry* entries, const BatchQueue& queue,
                                cudaStream_t stream, bool configure);
+
+// ---- flow engine: per-instance progress ----------------------------------------------------------------
+// One persistent kernel per bucket runs every iteration of the bucket's instances.  Each instance moves
+// through epochs e = 2 * iteration + phase (phase 0: descents, phase 1: perturbation + rebuild); a block claims
+// the next slot of the heaviest instance that has one, runs it, and the block that completes an epoch's last
+// slot finishes the epoch for the instance: after the descents the record (and stop rule), after the rebuilds
+// the iteration count, then publishes the next epoch.  No instance waits for another.
+struct FlowState {
+  unsigned long long claim;  // (epoch << 32) | next slot of the epoch; slot field >= population: none left
+  int32_t done;              // slots of the epoch completed
+  int32_t finished;          // the instance stopped: its record is final
+  unsigned long long t_done_ns;  // %globaltimer when it stopped
+};
+
+struct FlowBucket {
+  const int32_t* members;    // entry indices, heaviest first
+  int32_t count;
+  int32_t* remaining;        // unfinished members (the kernel ends at 0)
+  int32_t* error;            // kErrorWaitTimeout when a block found no work for idle_limit_ns
+  unsigned long long idle_limit_ns;
+};
+
+// Flow states of a bucket's members from their control blocks; `withheld` (may be null) marks instances whose
+// work is never published (a host-side fault injection for the bounded idle wait).
+cudaError_t LaunchFlowInit(const BatchEntry* entries, FlowState* flow, const FlowBucket& bucket,
+                           const int32_t* withheld, cudaStream_t stream);
+cudaError_t LaunchBatchFlow(const BatchShape& shape, const BatchEntry* entries, FlowState* flow,
+                            const FlowBucket& bucket, cudaStream_t stream, bool configure);
 // Occupancy of the bucket's kernel (blocks per SM at its shared memory), for sizing the persistent grid.
 int BatchDescentBlocksPerSm(const BatchShape& shape);
 cudaError_t LaunchBatchRebuild(const BatchEntry* entries, const BatchQueue& queue, int grid, cudaStream_t stream);

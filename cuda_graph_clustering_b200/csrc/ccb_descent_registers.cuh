@@ -50,58 +50,32 @@ __device__ __forceinline__ void LanesMinMax(const int* x, int& lo, int& hi) {
 //     kmin - kmax + ((P + 1 + 2^B) << S) + (u << 8) = ((gain + 2^B) << S) | (u << 8) | (a << 4) | to,
 // gain + 2^B in [2, 2^(B+1)) since the gain is in [1 - n, n - 1]: smaller gain, then smaller vertex, as the
 // reference orders moves, with both clusters riding in the low byte.  A move (v: from -> to) changes lanes
-// `from` and `to` of every vertex by -/+ 2^S (sign by adjacency to v); the block dispatches once per move on
-// (from, to) to a scan that touches only those two lanes.  Keys are unsigned so that the lanes of absent
-// vertices (u >= n, ignored) wrap instead of overflowing.
+// `from` and `to` of every vertex by -/+ 2^S (sign by adjacency to v), folded into the next scan.  Keys are
+// unsigned so that the lanes of absent vertices (u >= n, ignored) wrap instead of overflowing.
 constexpr int kCompactMaxBits = 10;
 
-template <int K, int V, int kFrom, int kTo>
+// One scan of the vertices: fold the last move into lanes (coef[c] = [c = from] - [c = to] times the signed step,
+// by adjacency to the moved vertex), then each vertex's move key.
+template <int K, int V>
 __device__ __forceinline__ uint32_t CompactScan(uint32_t (&key)[V][K], const uint32_t (&rw)[V], uint32_t lane_bit,
-                                                const uint32_t (&cu)[V], unsigned valid, uint32_t step) {
+                                                const uint32_t (&cu)[V], unsigned valid, const int (&coef)[K],
+                                                int step) {
   uint32_t best = ~0u;
 #pragma unroll
   for (int j = 0; j < V; ++j) {
-    if constexpr (kFrom >= 0) {
-      const uint32_t d = (rw[j] & lane_bit) ? step : 0u - step;
-      key[j][kFrom] += d;
-      key[j][kTo] -= d;
-    }
+    const int d = (rw[j] & lane_bit) ? step : -step;
     int lanes[K];
 #pragma unroll
-    for (int c = 0; c < K; ++c) lanes[c] = static_cast<int>(key[j][c]);
+    for (int c = 0; c < K; ++c) {
+      key[j][c] += static_cast<uint32_t>(coef[c] * d);
+      lanes[c] = static_cast<int>(key[j][c]);
+    }
     int kmin, kmax;
     LanesMinMax<K>(lanes, kmin, kmax);
     const uint32_t mk = static_cast<uint32_t>(kmin - kmax) + cu[j];
     best = min(best, ((valid >> j) & 1) ? mk : ~0u);
   }
   return best;
-}
-
-// The scan of the move (from, to) with both lanes known at compile time: one uniform jump per move.
-template <int K, int V>
-__device__ __forceinline__ uint32_t CompactScanMove(int from, int to, uint32_t (&key)[V][K], const uint32_t (&rw)[V],
-                                                    uint32_t lane_bit, const uint32_t (&cu)[V], unsigned valid,
-                                                    uint32_t step) {
-#define CCB_COMPACT_TO(F, T)                                                 \
-  case T:                                                                    \
-    if constexpr ((F) < K && (T) < K && (F) != (T)) {                        \
-      return CompactScan<K, V, F, T>(key, rw, lane_bit, cu, valid, step);    \
-    }                                                                        \
-    break;
-#define CCB_COMPACT_FROM(F)                                                                                    \
-  case F:                                                                                                      \
-    switch (to) {                                                                                              \
-      CCB_COMPACT_TO(F, 0) CCB_COMPACT_TO(F, 1) CCB_COMPACT_TO(F, 2) CCB_COMPACT_TO(F, 3)                      \
-      CCB_COMPACT_TO(F, 4) CCB_COMPACT_TO(F, 5) CCB_COMPACT_TO(F, 6) CCB_COMPACT_TO(F, 7)                      \
-    }                                                                                                          \
-    break;
-  switch (from) {
-    CCB_COMPACT_FROM(0) CCB_COMPACT_FROM(1) CCB_COMPACT_FROM(2) CCB_COMPACT_FROM(3)
-    CCB_COMPACT_FROM(4) CCB_COMPACT_FROM(5) CCB_COMPACT_FROM(6) CCB_COMPACT_FROM(7)
-  }
-#undef CCB_COMPACT_FROM
-#undef CCB_COMPACT_TO
-  return ~0u;  // not reached: from != to, both < K
 }
 
 template <int K, int T, int V>
@@ -152,9 +126,12 @@ __device__ __forceinline__ void DescentRegistersCompact(const DescentArgs<int16_
   const uint32_t vmask = (1u << bits) - 1u;
 
   uint32_t rw[V];
+  int coef[K];
 #pragma unroll
   for (int j = 0; j < V; ++j) rw[j] = 0u;
-  uint32_t best = CompactScan<K, V, -1, -1>(key, rw, lane_bit, cu, valid, step);
+#pragma unroll
+  for (int c = 0; c < K; ++c) coef[c] = 0;
+  uint32_t best = CompactScan<K, V>(key, rw, lane_bit, cu, valid, coef, static_cast<int>(step));
   while (true) {
     const uint32_t mkey = BlockArgMin<uint32_t, kWarps>(best, 0u, s_records + parity * kWarps).key;
     if (mkey >= no_move) break;
@@ -184,7 +161,9 @@ __device__ __forceinline__ void DescentRegistersCompact(const DescentArgs<int16_
     const uint32_t* row = rows + static_cast<size_t>(v) * a.gr.pitch;
 #pragma unroll
     for (int j = 0; j < V; ++j) rw[j] = ((valid >> j) & 1) ? row[(tid + j * T) >> 5] : 0u;  // words < ceil(n/32)
-    best = CompactScanMove<K, V>(from, to, key, rw, lane_bit, cu, valid, step);
+#pragma unroll
+    for (int c = 0; c < K; ++c) coef[c] = (c == from ? 1 : 0) - (c == to ? 1 : 0);
+    best = CompactScan<K, V>(key, rw, lane_bit, cu, valid, coef, static_cast<int>(step));
   }
 
   uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;

@@ -33,6 +33,8 @@ static __global__ void k_mark_start(Control* ctl) {
   ctl->t0_ns = GlobalTimerNs();
 }
 
+static __global__ void k_clock(unsigned long long* t) { *t = GlobalTimerNs(); }
+
 static __global__ void k_degrees(const uint32_t* __restrict__ bits, int n, int words, int pitch, int32_t* degrees) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
@@ -81,8 +83,9 @@ template <typename GainT, int kThreads>
 __device__ __forceinline__ void RebuildBody(const RebuildArgs<GainT>& a, int slot) {
   const GraphView& gr = a.gr;
   const PopView<GainT>& cur = a.cur;
-  const uint8_t* __restrict__ next_labels = a.next_labels;
-  const int32_t* __restrict__ src_map = a.src_map;
+  // plain (coherent) loads: in the batched flow kernel these are written by other blocks of the same launch
+  const uint8_t* next_labels = a.next_labels;
+  const int32_t* src_map = a.src_map;
   uint32_t* __restrict__ masks = a.masks;
   const int k = a.k, kpad = a.kpad, ld = a.ld, mode = a.mode;
   const uint64_t stream = a.stream;

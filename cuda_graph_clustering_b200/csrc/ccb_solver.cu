@@ -963,6 +963,13 @@ struct ccb_batch {
   int max_iterations = 0;
   long long replays = 0;
   double l2_share = 0.0;  // 0: persistent grids fill every SM (see BuildWorkLists)
+  int engine = CCB_BATCH_FLOW;
+  double wait_limit_sec = 30.0;        // flow engine: a block's idle wait gives up after this long
+  std::vector<int32_t> withheld;       // per instance: its flow work is never published (fault injection)
+  FlowState* d_flow = nullptr;         // per entry
+  int32_t* d_flow_counters = nullptr;  // remaining per bucket, then the error flag
+  int32_t* d_withheld = nullptr;       // per entry
+  unsigned long long* d_t0 = nullptr;  // %globaltimer at the start of a flow run
 
   ~ccb_batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -973,6 +980,10 @@ struct ccb_batch {
     if (d_entries) cudaFree(d_entries);
     if (d_active) cudaFree(d_active);
     if (h_active) cudaFreeHost(h_active);
+    if (d_flow) cudaFree(d_flow);
+    if (d_flow_counters) cudaFree(d_flow_counters);
+    if (d_withheld) cudaFree(d_withheld);
+    if (d_t0) cudaFree(d_t0);
   }
 };
 
@@ -1155,6 +1166,7 @@ void BuildWorkLists(WorkLists& w, const std::vector<const ccb_solver*>& solvers,
     if (bk.shape.max_slots > 0) grid = std::min<long long>(grid, bk.shape.max_slots);
     bk.shape.grid = (int)std::max<long long>(1, std::min<long long>(grid, bk.total));
     CCB_CUDA(LaunchBatchDescent(bk.shape, nullptr, BatchQueue{}, nullptr, true));
+    CCB_CUDA(LaunchBatchFlow(bk.shape, nullptr, nullptr, FlowBucket{}, nullptr, true));
     CCB_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
     CCB_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
     char line[200];
@@ -1234,6 +1246,17 @@ void PrepareBatch(ccb_batch& b) {
     CCB_CUDA(cudaMemcpy(b.d_entries, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice));
   }
   for (cudaEvent_t& e : b.poll) CCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (b.engine == CCB_BATCH_FLOW) {
+    CCB_CUDA(cudaMalloc(&b.d_flow, std::max(1, count) * sizeof(FlowState)));
+    CCB_CUDA(cudaMalloc(&b.d_flow_counters, (b.work.buckets.size() + 1) * sizeof(int32_t)));
+    CCB_CUDA(cudaMalloc(&b.d_t0, sizeof(unsigned long long)));
+    std::vector<int32_t> held(std::max(1, count), 0);
+    for (int e = 0; e < count; ++e) held[e] = b.withheld[b.batched[e]];
+    CCB_CUDA(cudaMalloc(&b.d_withheld, held.size() * sizeof(int32_t)));
+    CCB_CUDA(cudaMemcpy(b.d_withheld, held.data(), held.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    b.prepared = true;
+    return;
+  }
   // One PBILS iteration of every instance, captured once as a graph and replayed.
   if (count > 0) {
     CCB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
@@ -1270,6 +1293,47 @@ void EnqueueInit(ccb_solver& s, const ccb_params& p, cudaStream_t st) {
   }
 }
 
+// The flow engine's run: one persistent kernel per bucket, each on its stream, carrying its instances through
+// all their iterations; returns the device clock at the start (for per-instance completion times).
+unsigned long long RunFlow(ccb_batch& b, std::vector<FlowState>& states) {
+  const cudaStream_t st = b.stream;
+  const int count = (int)b.batched.size();
+  WorkLists& w = b.work;
+  const int nb = (int)w.buckets.size();
+  CCB_CUDA(cudaMemsetAsync(b.d_flow_counters, 0, (nb + 1) * sizeof(int32_t), st));
+  std::vector<FlowBucket> fb(nb);
+  for (int i = 0; i < nb; ++i) {
+    fb[i].members = w.d_lists + w.buckets[i].offset;
+    fb[i].count = (int32_t)w.buckets[i].members.size();
+    fb[i].remaining = b.d_flow_counters + i;
+    fb[i].error = b.d_flow_counters + nb;
+    fb[i].idle_limit_ns = (unsigned long long)(std::max(1e-3, b.wait_limit_sec) * 1e9);
+    CCB_CUDA(LaunchFlowInit(b.d_entries, b.d_flow, fb[i], b.d_withheld, st));
+  }
+  k_clock<<<1, 1, 0, st>>>(b.d_t0);
+  CCB_CUDA(cudaGetLastError());
+  CCB_CUDA(cudaEventRecord(w.fork, st));
+  for (int i = 0; i < nb; ++i) {
+    WorkLists::Bucket& bk = w.buckets[i];
+    CCB_CUDA(cudaStreamWaitEvent(bk.stream, w.fork, 0));
+    CCB_CUDA(LaunchBatchFlow(bk.shape, b.d_entries, b.d_flow, fb[i], bk.stream, false));
+    CCB_CUDA(cudaEventRecord(bk.done, bk.stream));
+    CCB_CUDA(cudaStreamWaitEvent(st, bk.done, 0));
+  }
+  int32_t error = 0;
+  unsigned long long t0 = 0;
+  states.resize(std::max(1, count));
+  CCB_CUDA(cudaMemcpyAsync(&error, b.d_flow_counters + nb, sizeof(error), cudaMemcpyDeviceToHost, st));
+  CCB_CUDA(cudaMemcpyAsync(&t0, b.d_t0, sizeof(t0), cudaMemcpyDeviceToHost, st));
+  CCB_CUDA(cudaMemcpyAsync(states.data(), b.d_flow, count * sizeof(FlowState), cudaMemcpyDeviceToHost, st));
+  CCB_CUDA(cudaStreamSynchronize(st));
+  if (error == kErrorWaitTimeout) {
+    Fail(CCB_ERR_TIMEOUT, "batched flow engine: a block found no work to claim for the wait limit (" +
+                              std::to_string(b.wait_limit_sec) + " s) while instances were unfinished");
+  }
+  return t0;
+}
+
 void RunBatch(ccb_batch& b) {
   TraceRange trace_range("ccb.batch.run");
   const auto started = std::chrono::steady_clock::now();
@@ -1279,7 +1343,10 @@ void RunBatch(ccb_batch& b) {
     ccb_batch::Instance& in = b.inst[b.batched[e]];
     EnqueueInit(*in.solver, in.params, st);
   }
-  if (b.exec != nullptr) {
+  std::vector<FlowState> states;
+  unsigned long long flow_t0 = 0;
+  if (b.engine == CCB_BATCH_FLOW && !b.batched.empty()) flow_t0 = RunFlow(b, states);
+  if (b.engine == CCB_BATCH_LOCKSTEP && b.exec != nullptr) {
     int chunk = 0;
     for (int r = 0; r < b.max_iterations; ++r) {
       CCB_CUDA(cudaGraphLaunch(b.exec, st));
@@ -1320,6 +1387,10 @@ void RunBatch(ccb_batch& b) {
     in.result.accepted_moves = (int64_t)c.moves;
     in.result.clusters_used = CountClustersUsed(in.labels.data(), (uint32_t)s.n, s.k);
     in.result.seconds = seconds;
+    if (b.engine == CCB_BATCH_FLOW) {  // this instance's own completion, from the start of the run
+      const FlowState& f = states[b.entry_of[i]];
+      in.result.seconds = f.t_done_ns > flow_t0 ? (double)(f.t_done_ns - flow_t0) * 1e-9 : 0.0;
+    }
   }
 }
 
@@ -1853,6 +1924,7 @@ int ccb_batch_add(ccb_batch* b, const ccb_graph* g, const ccb_params* params, in
     in.graph = g;
     in.params = *params;
     b->inst.push_back(std::move(in));
+    b->withheld.push_back(0);
     if (id_out) *id_out = (int32_t)b->inst.size() - 1;
   });
 }
@@ -1871,6 +1943,26 @@ int ccb_batch_result(const ccb_batch* b, int32_t id, int32_t* labels_out, ccb_re
     const ccb_batch::Instance& in = b->inst[id];
     *result = in.result;
     if (labels_out && !in.labels.empty()) std::memcpy(labels_out, in.labels.data(), in.labels.size() * 4);
+  });
+}
+
+int ccb_batch_set_engine(ccb_batch* b, int32_t engine, double wait_limit_sec) {
+  return Guard([&] {
+    if (!b) Fail(CCB_ERR_STATE, "null batch");
+    if (b->prepared) Fail(CCB_ERR_STATE, "batch already prepared: set the engine before the first run");
+    if (engine != CCB_BATCH_FLOW && engine != CCB_BATCH_LOCKSTEP) Fail(CCB_ERR_INVALID, "unknown batch engine");
+    if (wait_limit_sec < 0) Fail(CCB_ERR_INVALID, "wait limit must be >= 0");
+    b->engine = engine;
+    b->wait_limit_sec = wait_limit_sec > 0 ? wait_limit_sec : 30.0;
+  });
+}
+
+int ccb_batch_withhold(ccb_batch* b, int32_t id) {
+  return Guard([&] {
+    if (!b) Fail(CCB_ERR_STATE, "null batch");
+    if (b->prepared) Fail(CCB_ERR_STATE, "batch already prepared");
+    if (id < 0 || id >= (int32_t)b->inst.size()) Fail(CCB_ERR_STATE, "no such instance");
+    b->withheld[id] = 1;
   });
 }
 

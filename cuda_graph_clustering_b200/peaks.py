@@ -3,8 +3,8 @@
     python -m cuda_graph_clustering_b200.peaks > profiles/peaks_l2_hbm.txt
 
 A device-to-device copy (read + write, both counted) of a buffer pair, timed with CUDA events over many
-repetitions after a warm-up: pairs of 2 x 8 / 16 / 24 MiB stay in the 126 MB L2 between repetitions (the L2
-figure is their best), a pair of 2 x 2 GiB streams from HBM.  A dense int8 GEMM (cuBLASLt) gives the int8
+repetitions after a warm-up: pairs of 2 x 16 / 32 / 48 MiB stay in the 126 MB L2 between repetitions (their
+copies captured in one CUDA graph; the L2 figure is their best), a pair of 2 x 2 GiB streams from HBM.  A dense int8 GEMM (cuBLASLt) gives the int8
 tensor-core peak of the tensor rebuild's roofline.  The driver-written HBM figure (a STREAM-style
 copy) is the HBM peak of record; this one is printed beside it as a cross-check.  One JSON object per line,
 then a summary line that bench.py reads ("l2_copy_gbs: ...").
@@ -14,16 +14,33 @@ from __future__ import annotations
 import json
 
 
-def copy_gbs(torch, nbytes: int, reps: int) -> float:
+def copy_gbs(torch, nbytes: int, reps: int, graph: bool = False) -> float:
+    """Read + write bandwidth of `reps` back-to-back copies; with `graph` they are captured in one CUDA graph so
+    that host launch gaps do not count (the L2-resident copies last only microseconds each)."""
     src = torch.empty(nbytes, dtype=torch.uint8, device="cuda").fill_(1)
     dst = torch.empty_like(src)
     for _ in range(5):
         dst.copy_(src)
+    run = None
+    if graph:
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(g):
+                for _ in range(reps):
+                    dst.copy_(src)
+        torch.cuda.current_stream().wait_stream(side)
+        g.replay()
+        run = g.replay
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     start.record()
-    for _ in range(reps):
-        dst.copy_(src)
+    if run is not None:
+        run()
+    else:
+        for _ in range(reps):
+            dst.copy_(src)
     stop.record()
     torch.cuda.synchronize()
     ms = start.elapsed_time(stop)
@@ -51,8 +68,8 @@ def main() -> None:
 
     props = torch.cuda.get_device_properties(0)
     l2 = []
-    for mib in (8, 16, 24):
-        gbs = copy_gbs(torch, mib << 20, 2000)
+    for mib in (16, 32, 48):
+        gbs = copy_gbs(torch, mib << 20, 500, graph=True)
         l2.append(gbs)
         print(json.dumps({"buffer_pair_mib": 2 * mib, "copy_gbs": round(gbs, 1), "resident": "L2"}))
     hbm = copy_gbs(torch, 2 << 30, 20)

@@ -166,17 +166,30 @@ int ccb_solver_stats(const ccb_solver* solver, ccb_kernel_stats* stats);
 
 /* ---- batched solves ----------------------------------------------------------------------------
  * No counterpart in the reference (which solves one instance per call).  Many independent PBILS instances
- * (each its own graph, k, population, seed, ...) run together: every iteration of all instances is one
- * CUDA graph replay whose descent phase is a persistent kernel per shape bucket, draining a device queue of
- * (instance, slot) work items; record, GWW and perturbation+rebuild follow as one kernel each.  Results
- * are the same as ccb_solver_pbils / ccb_pbils_solve would give each instance alone, bit for bit.
+ * (each its own graph, k, population, seed, ...) run together in persistent kernels, one per shape bucket,
+ * that pull (instance, slot) work items from device queues (see ccb_batch_set_engine).  Results are the
+ * same as ccb_solver_pbils / ccb_pbils_solve would give each instance alone, bit for bit.
  * Graphs are device-resident (ccb_graph_upload) and must outlive the batch.  Instances with k = 1 or
  * n > 32767 are solved one by one on the plain path after the batched ones. */
 typedef struct ccb_batch ccb_batch;
 int ccb_batch_create(ccb_batch** out);
 int ccb_batch_add(ccb_batch* batch, const ccb_graph* graph, const ccb_params* params, int32_t* id_out);
-/* Solves every instance (again on each call: same inputs, same results).  Synchronous. */
+/* Solves every instance (again on each call: same inputs, same results).  Synchronous.  Each result's `seconds`
+ * is the instance's own completion time from the start of the run under the flow engine, the run's time under
+ * the lock-step engine. */
 int ccb_batch_run(ccb_batch* batch);
+/* The engine, chosen before the first run.  CCB_BATCH_FLOW (default): one persistent kernel per shape bucket
+ * carries every instance through all its iterations; a block claims the next (instance, slot) item of the
+ * heaviest instance that has one, and the block that completes an instance's last descent (rebuild) slot runs
+ * its record and stop rule (advances its iteration) and publishes its next phase, so no instance waits for
+ * another.  A block that finds nothing to claim while instances are unfinished sleeps, and gives up after
+ * wait_limit_sec (0: 30 s) with CCB_ERR_TIMEOUT.  CCB_BATCH_LOCKSTEP: one CUDA graph replay per iteration of
+ * all instances. */
+enum ccb_batch_engine { CCB_BATCH_FLOW = 0, CCB_BATCH_LOCKSTEP = 1 };
+int ccb_batch_set_engine(ccb_batch* batch, int32_t engine, double wait_limit_sec);
+/* Host-side fault injection for tests of the bounded wait: instance `id`'s work is never published to the flow
+ * engine's blocks, so the run ends in CCB_ERR_TIMEOUT after the wait limit instead of waiting forever. */
+int ccb_batch_withhold(ccb_batch* batch, int32_t id);
 int ccb_batch_result(const ccb_batch* batch, int32_t id, int32_t* labels_out, ccb_result* result);
 /* Text description of the buckets (kernel, shape, instances, slots, persistent grid). */
 const char* ccb_batch_describe(const ccb_batch* batch);

@@ -71,6 +71,60 @@ def test_batch_matches_plain_and_oracle(ccb, oracle, cuda_device):
     assert [batch.result(i).objective for i in ids] == first
 
 
+def test_lockstep_engine_matches_flow_engine(ccb, cuda_device):
+    """The lock-step engine (one graph replay per iteration of all instances) and the flow engine (each instance
+    on its own) give every instance the same result."""
+    runs = []
+    for engine in ("lockstep", "flow"):
+        batch = ccb.Batch(engine=engine)
+        ids = []
+        for i, (n, k, pop, gww, tour, iters, early, pert, seed) in enumerate(MIX):
+            dg, _ = ccb.DeviceGraph.planted(n, max(2, k // 2), 0.5, 0.05, 0.1, 400 + i)
+            ids.append(batch.add(dg, ccb.PbilsParams(k=k, population=pop, gww=gww, tournament=tour, iterations=iters,
+                                                     early_stop=early, perturbation=pert, seed=seed)))
+        batch.run()
+        runs.append([batch.result(i) for i in ids])
+        batch.close()
+    for a, b in zip(*runs):
+        assert _results_equal(a, b)
+
+
+def test_flow_engine_bounded_wait_ends_with_timeout(ccb, cuda_device):
+    """Host-side fault injection: one instance's work is never published, so the other instances finish and then
+    every block of its bucket finds nothing to claim; after the 1 s wait limit the kernel gives up (no trap, no
+    endless spin) and the run reports CCB_ERR_TIMEOUT.  The device stays usable for the next batch."""
+    from cuda_graph_clustering_b200._native import CCB_ERR_TIMEOUT, CcbError
+    batch = ccb.Batch(engine="flow", wait_limit_sec=1.0)
+    graphs = [ccb.DeviceGraph.planted(300 + 50 * i, 3, 0.5, 0.05, 0.1, 500 + i)[0] for i in range(4)]
+    for g in graphs:
+        batch.add(g, ccb.PbilsParams(k=4, population=16, iterations=5, early_stop=5, seed=2))
+    batch.withhold(2)
+    with pytest.raises(CcbError) as e:
+        batch.run()
+    assert e.value.status == CCB_ERR_TIMEOUT and "wait limit" in str(e.value)
+    batch.close()
+    again = ccb.Batch(engine="flow", wait_limit_sec=1.0)
+    ids = [again.add(g, ccb.PbilsParams(k=4, population=16, iterations=5, early_stop=5, seed=2)) for g in graphs]
+    again.run()
+    for g, i in zip(graphs, ids):
+        assert _results_equal(again.result(i), ccb.SolveGpu(g.download(), ccb.PbilsParams(
+            k=4, population=16, iterations=5, early_stop=5, seed=2)))
+
+
+def test_flow_engine_reports_per_instance_completion(ccb, cuda_device):
+    """Under the flow engine a small instance finishes long before a large one: its own completion time is
+    reported, not the run's."""
+    batch = ccb.Batch(engine="flow")
+    small = batch.add(ccb.DeviceGraph.planted(200, 2, 0.5, 0.05, 0.1, 601)[0],
+                      ccb.PbilsParams(k=3, population=32, iterations=3, early_stop=3, seed=1))
+    large = batch.add(ccb.DeviceGraph.planted(12000, 8, 0.5, 0.05, 0.1, 602)[0],
+                      ccb.PbilsParams(k=20, population=64, iterations=20, early_stop=20, seed=1))
+    batch.run()
+    ts, tl = batch.result(small).seconds, batch.result(large).seconds
+    assert 0 < ts < tl
+    assert ts < 0.5 * tl
+
+
 @pytest.mark.parametrize("table", [
     [dict(kind=-1, n_min=0, n_max=1 << 20, k_min=0, k_max=64, use_kind=2, threads=256, blocks_per_sm=0,
           max_slots=0)],
