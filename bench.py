@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving", "neighborhood"],
                     default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rebuild", choices=["auto", "popcount", "tensor"], default="auto",
+                    help="wide workloads: how G = A*Z is rebuilt (the tensor path is timed beside the popcount one)")
     ap.add_argument("--batch-count", type=int, default=256, help="batched workload: instances")
     ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
     ap.add_argument("--batch-engine", choices=["flow", "lockstep"], default="flow", help="batched workload: engine")
@@ -664,6 +666,8 @@ def main():
     sh = stream.cuda_stream
     dg = ccb.DeviceGraph(graph, stream=sh)
     solver = ccb.Solver(dg, params)
+    if args.rebuild != "auto":
+        solver.set_rebuild(args.rebuild)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     expected = objectives.get(seed)
 
@@ -700,6 +704,19 @@ def main():
     solver.set_profiling(True)
     prof = solver.pbils(params, stream=sh, want_labels=False)
     st = solver.stats()
+    rebuild_compare = None
+    if "tensor cores" in solver.describe():
+        # the same solve with the popcount rebuild: identical trajectory, the rebuild phase timed beside
+        solver.set_rebuild("popcount")
+        alt = solver.pbils(params, stream=sh, want_labels=False)
+        st_pop = solver.stats()
+        solver.set_rebuild(args.rebuild)
+        n_, k_, pop_ = cfg["n"], cfg["k"], cfg["population"]
+        ops = 2.0 * n_ * n_ * pop_ * k_ * st.rebuild_launches  # int8 MACs x 2 of every rebuild (initial included)
+        rebuild_compare = {"tensor_ms_per_solve": st.rebuild_ms, "popcount_ms_per_solve": st_pop.rebuild_ms,
+                           "launches": st.rebuild_launches, "same_objective": alt.objective == prof.objective,
+                           "tensor_phase_tops": ops / (st.rebuild_ms * 1e-3) / 1e12,
+                           "note": "rebuild phase = labels/masks/sizes + one-hot Z + tcgen05 contraction + f"}
     solver.set_profiling(False)
     descent_ms = st.descent_ms / max(st.descent_launches, 1)
     launches_per_solve = st.descent_launches + st.rebuild_launches + st.record_launches + st.other_launches
@@ -810,6 +827,7 @@ def main():
             "clocks": clock_info,
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "rebuild_tensor_vs_popcount": rebuild_compare,
         }
         print(json.dumps(line))
     if dist is not None:

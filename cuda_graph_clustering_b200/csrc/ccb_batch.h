@@ -64,7 +64,7 @@ struct FlowState {
 struct FlowBucket {
   const int32_t* members;    // entry indices, heaviest first
   int32_t count;
-  int32_t* remaining;        // unfinished members (the kernel ends at 0)
+  int32_t* remaining;        // [0] unfinished members (the kernel ends at 0), [1] their slots, [2] running blocks
   int32_t* error;            // kErrorWaitTimeout when a block found no work for idle_limit_ns
   unsigned long long idle_limit_ns;
 };

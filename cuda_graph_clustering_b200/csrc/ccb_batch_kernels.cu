@@ -148,6 +148,7 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
   __shared__ int s_entry, s_slot, s_flag;
   __shared__ unsigned long long s_epoch;
   unsigned long long idle_since = 0;
+  if (threadIdx.x == 0) atomicAdd(b.remaining + 2, 1);
   for (;;) {
     if (threadIdx.x == 0) {
       s_entry = -1;
@@ -172,6 +173,10 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
         idle_since = 0;
       } else if (LoadAcquire(b.remaining) <= 0 || LoadAcquire(b.error) != 0) {
         s_flag = 1;  // the bucket is done (or gave up): leave
+      } else if (LoadAcquire(b.remaining + 2) > LoadAcquire(b.remaining + 1)) {
+        // more blocks run than the unfinished instances have slots: this one is never needed again, and its SM is
+        // freed for the other buckets
+        s_flag = 1;
       } else {
         const unsigned long long now = GlobalTimerNs();
         if (idle_since == 0) {
@@ -185,7 +190,10 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
     }
     __syncthreads();
     if (s_entry < 0) {
-      if (s_flag) break;
+      if (s_flag) {
+        if (threadIdx.x == 0) atomicSub(b.remaining + 2, 1);
+        break;
+      }
       continue;
     }
     const int e = s_entry, slot = s_slot;
@@ -231,6 +239,7 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
         flow[e].finished = 1;
         __threadfence();
         atomicExch(&flow[e].claim, ((epoch + 1) << 32) | kFlowNone);
+        atomicSub(b.remaining + 1, E.descent.population);
         atomicSub(b.remaining, 1);
       } else {
         __threadfence();
@@ -278,7 +287,10 @@ __global__ void kb_flow_init(const BatchEntry* __restrict__ entries, FlowState* 
   f.t_done_ns = 0;
   f.finished = stopped ? 1 : 0;
   f.claim = (stopped || (withheld != nullptr && withheld[e])) ? kFlowNone : 0ull;
-  if (!stopped) atomicAdd(b.remaining, 1);
+  if (!stopped) {
+    atomicAdd(b.remaining, 1);
+    atomicAdd(b.remaining + 1, entries[e].descent.population);
+  }
 }
 
 template <typename Kernel>

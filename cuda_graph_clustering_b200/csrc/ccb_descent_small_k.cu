@@ -2,6 +2,7 @@
 // so that the many template instances compile in parallel with the rest of the library.
 #include <cuda_runtime.h>
 
+#include "ccb_descent_cluster.cuh"
 #include "ccb_descent_incremental.cuh"
 #include "ccb_descent_registers.cuh"
 #include "ccb_descent_stream.cuh"
@@ -15,6 +16,15 @@ cudaError_t GoStream(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaS
   auto kernel = k_descent_stream<K, T, S>;
   if (configure) return RaiseDynamicSmem(kernel, smem);
   kernel<<<grid, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int K, int C>
+cudaError_t GoCluster(const DescentArgs<int16_t>& a, int slots, size_t smem, cudaStream_t st, bool configure) {
+  auto kernel = k_descent_cluster<K, 1024, C>;
+  if (configure) return RaiseDynamicSmem(kernel, smem);
+  if (slots <= 0) return cudaSuccess;
+  kernel<<<slots * C, 1024, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -49,6 +59,13 @@ cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int 
   if (p.registers) {
     return p.smem_rows ? RegistersByShape<K, true>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg)
                        : RegistersByShape<K, false>(p.threads, p.vpt, a, grid, p.smem_bytes, st, cfg);
+  }
+  if (p.cluster > 0) {
+    switch (p.cluster) {
+      case 2: return GoCluster<K, 2>(a, grid, p.smem_bytes, st, cfg);
+      case 4: return GoCluster<K, 4>(a, grid, p.smem_bytes, st, cfg);
+      default: return GoCluster<K, 8>(a, grid, p.smem_bytes, st, cfg);
+    }
   }
   if (p.threads == 512) {
     return p.smem_state ? GoStream<K, 512, true>(a, grid, p.smem_bytes, st, cfg)
@@ -133,6 +150,17 @@ size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state,
 }
 
 int SmallKLanes(int k) { return PackedLanes(k); }
+
+int StreamCluster(int k, int n, size_t limit, size_t* bytes_per_cta) {
+  for (int c = 2; c <= 8; c *= 2) {
+    const size_t bytes = (size_t)ClusterSpan(n, c) * PackedLanes(k) * 2;
+    if (bytes <= limit) {
+      *bytes_per_cta = bytes;
+      return c;
+    }
+  }
+  return 0;
+}
 
 size_t RegistersSmem(int n, int pitch, bool smem_rows) {
   return smem_rows ? ((size_t)n * pitch * 4 + 15) / 16 * 16 : 0;

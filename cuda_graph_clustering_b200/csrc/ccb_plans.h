@@ -18,7 +18,11 @@ struct SmallKPlan {
   bool smem_state = false;  // packed G + labels in shared memory (else the slot's rows of `next`)
   bool smem_rows = false;   // whole bitset in shared memory
   size_t smem_bytes = 0;
+  int cluster = 0;          // streamed form whose state does not fit one CTA: CTAs of the cluster holding it
 };
+// The smallest cluster (2, 4 or 8 CTAs) whose shares of the packed state fit `limit` bytes of shared memory per
+// CTA, with its bytes per CTA; 0 if none.
+int StreamCluster(int k, int n, size_t limit, size_t* bytes_per_cta);
 
 size_t SmallKSmem(int k, int n, int pitch, int ld, int threads, bool smem_state, bool smem_rows);
 int SmallKLanes(int k);

@@ -207,6 +207,9 @@ size_t DescentSmem(const Plan& p, int n, int pitch, int k, int ld, int kpad) {
 }
 
 constexpr int kMaxVerticesIncrementalWide = 65536;
+// The streamed K <= 8 descent with its state in a thread-block cluster's shared memory when it does not fit one
+// CTA (else it streams from L2).
+constexpr bool kClusterDescent = true;
 
 Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const Device& dev) {
   Plan p;
@@ -243,6 +246,13 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
       sk.smem_state = SmallKSmem(k, n, pitch, ld, sk.threads, true, false) <= limit;
       sk.smem_rows = false;
       sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, false);
+      if (!sk.smem_state && kClusterDescent) {
+        // the state spread over a cluster's shared memory instead of streaming from L2 (the batched engine
+        // keeps the L2 form: its buckets are one CTA per slot)
+        size_t per_cta = 0;
+        sk.cluster = StreamCluster(k, n, limit - 4096, &per_cta);
+        if (sk.cluster > 0) sk.smem_bytes = per_cta;
+      }
     }
     p.small_k = true;
     p.smem_state = sk.smem_state;
@@ -354,6 +364,7 @@ const char* KernelName(const Plan& p) {
   if (p.small_k) {
     if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
                                            : "packed k <= 8, registers";
+    if (p.sk.cluster > 0) return "packed k <= 8, state in the distributed shared memory of a CTA cluster";
     return p.smem_state ? "packed k <= 8, streamed from shared memory" : "packed k <= 8, streamed from L2";
   }
   if (p.wide) return "generic wide (int32 G), global memory";
@@ -488,7 +499,7 @@ namespace {
 void Describe(ccb_solver& s) {
   char text[320];
   std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory%s",
-                KernelName(s.plan), s.plan.threads, s.pop, s.plan.smem_bytes,
+                KernelName(s.plan), s.plan.threads, s.pop * std::max(1, s.plan.sk.cluster), s.plan.smem_bytes,
                 s.tensor ? "; G rebuilt on the tensor cores (int8 tcgen05, TMA)" : "");
   s.description = text;
 }
@@ -1077,7 +1088,7 @@ BatchShape ShapeOfPlan(const ccb_solver& s) {
     sh.kind = kBatchStream;
     sh.smem = sk.smem_state;
   }
-  sh.smem_bytes = sk.smem_bytes;
+  sh.smem_bytes = sk.cluster > 0 ? 0 : sk.smem_bytes;  // a cluster plan's batched form streams from L2
   return sh;
 }
 
@@ -1248,7 +1259,7 @@ void PrepareBatch(ccb_batch& b) {
   for (cudaEvent_t& e : b.poll) CCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (b.engine == CCB_BATCH_FLOW) {
     CCB_CUDA(cudaMalloc(&b.d_flow, std::max(1, count) * sizeof(FlowState)));
-    CCB_CUDA(cudaMalloc(&b.d_flow_counters, (b.work.buckets.size() + 1) * sizeof(int32_t)));
+    CCB_CUDA(cudaMalloc(&b.d_flow_counters, (3 * b.work.buckets.size() + 1) * sizeof(int32_t)));
     CCB_CUDA(cudaMalloc(&b.d_t0, sizeof(unsigned long long)));
     std::vector<int32_t> held(std::max(1, count), 0);
     for (int e = 0; e < count; ++e) held[e] = b.withheld[b.batched[e]];
@@ -1300,13 +1311,13 @@ unsigned long long RunFlow(ccb_batch& b, std::vector<FlowState>& states) {
   const int count = (int)b.batched.size();
   WorkLists& w = b.work;
   const int nb = (int)w.buckets.size();
-  CCB_CUDA(cudaMemsetAsync(b.d_flow_counters, 0, (nb + 1) * sizeof(int32_t), st));
+  CCB_CUDA(cudaMemsetAsync(b.d_flow_counters, 0, (3 * nb + 1) * sizeof(int32_t), st));
   std::vector<FlowBucket> fb(nb);
   for (int i = 0; i < nb; ++i) {
     fb[i].members = w.d_lists + w.buckets[i].offset;
     fb[i].count = (int32_t)w.buckets[i].members.size();
-    fb[i].remaining = b.d_flow_counters + i;
-    fb[i].error = b.d_flow_counters + nb;
+    fb[i].remaining = b.d_flow_counters + 3 * i;
+    fb[i].error = b.d_flow_counters + 3 * nb;
     fb[i].idle_limit_ns = (unsigned long long)(std::max(1e-3, b.wait_limit_sec) * 1e9);
     CCB_CUDA(LaunchFlowInit(b.d_entries, b.d_flow, fb[i], b.d_withheld, st));
   }
@@ -1323,7 +1334,7 @@ unsigned long long RunFlow(ccb_batch& b, std::vector<FlowState>& states) {
   int32_t error = 0;
   unsigned long long t0 = 0;
   states.resize(std::max(1, count));
-  CCB_CUDA(cudaMemcpyAsync(&error, b.d_flow_counters + nb, sizeof(error), cudaMemcpyDeviceToHost, st));
+  CCB_CUDA(cudaMemcpyAsync(&error, b.d_flow_counters + 3 * nb, sizeof(error), cudaMemcpyDeviceToHost, st));
   CCB_CUDA(cudaMemcpyAsync(&t0, b.d_t0, sizeof(t0), cudaMemcpyDeviceToHost, st));
   CCB_CUDA(cudaMemcpyAsync(states.data(), b.d_flow, count * sizeof(FlowState), cudaMemcpyDeviceToHost, st));
   CCB_CUDA(cudaStreamSynchronize(st));
