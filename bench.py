@@ -74,7 +74,8 @@ def parse():
                     help="wide workloads: how G = A*Z is rebuilt (the tensor path is timed beside the popcount one)")
     ap.add_argument("--batch-count", type=int, default=256, help="batched workload: instances")
     ap.add_argument("--batch-iters", type=int, default=100, help="batched workload: iterations per instance")
-    ap.add_argument("--batch-engine", choices=["flow", "lockstep"], default="flow", help="batched workload: engine")
+    ap.add_argument("--batch-engine", choices=["flow", "lockstep"], default="lockstep",
+                    help="batched workload: engine")
     ap.add_argument("--serve-count", type=int, default=32, help="serving workload: requests")
     ap.add_argument("--serve-rate", type=float, default=10.0, help="serving workload: Poisson arrivals per second")
     ap.add_argument("--serve-max-n", type=int, default=32767,

@@ -349,11 +349,11 @@ BATCH_ENGINES = {"flow": 0, "lockstep": 1}
 
 class Batch:
     """Many independent PBILS instances solved together (ccb_batch_*) by persistent per-bucket kernels fed by
-    device work queues: the flow engine (default; every instance advances on its own) or the lock-step engine
-    (one CUDA graph replay per iteration of all instances).  Each result equals the instance's plain solve bit
+    device work queues: the lock-step engine (default; one CUDA graph replay per iteration of all instances) or
+    the flow engine (every instance advances on its own).  Each result equals the instance's plain solve bit
     for bit."""
 
-    def __init__(self, engine: str = "flow", wait_limit_sec: float = 0.0):
+    def __init__(self, engine: str = "lockstep", wait_limit_sec: float = 0.0):
         _ensure_tuning()
         h = C.c_void_p()
         check(lib().ccb_batch_create(C.byref(h)))

@@ -39,6 +39,7 @@ cudaError_t GoRegisters(const DescentArgs<int16_t>& a, int grid, size_t smem, cu
 template <int K, bool R>
 cudaError_t RegistersByShape(int threads, int vpt, const DescentArgs<int16_t>& a, int grid, size_t smem,
                              cudaStream_t st, bool cfg) {
+  if (vpt == 16) return GoRegisters<K, 64, 16, R>(a, grid, smem, st, cfg);
   if (vpt == 8) {
     switch (threads) {
       case 128: return GoRegisters<K, 128, 8, R>(a, grid, smem, st, cfg);
@@ -167,7 +168,7 @@ size_t RegistersSmem(int n, int pitch, bool smem_rows) {
 }
 
 bool RegistersShapeBuilt(int threads, int vpt) {
-  return (vpt == 8 && (threads == 128 || threads == 256 || threads == 512)) ||
+  return (vpt == 16 && threads == 64) || (vpt == 8 && (threads == 128 || threads == 256 || threads == 512)) ||
          (vpt == 4 && (threads == 128 || threads == 256 || threads == 512 || threads == 1024));
 }
 

@@ -208,10 +208,12 @@ size_t DescentSmem(const Plan& p, int n, int pitch, int k, int ld, int kpad) {
 
 constexpr int kMaxVerticesIncrementalWide = 65536;
 // The streamed K <= 8 descent with its state in a thread-block cluster's shared memory when it does not fit one
-// CTA (else it streams from L2).
+// CTA, used when all the population's clusters run at once: a slot then moves ~1.8x faster than streaming its
+// state from L2, but takes C SMs instead of one, so with more slots than one wave of clusters the L2 form is
+// faster (n = 32000, k = 8, pop 128: 608 ms per descent launch in clusters of 4 against 322 ms streamed).
 constexpr bool kClusterDescent = true;
 
-Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const Device& dev) {
+Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const Device& dev, int pop) {
   Plan p;
   p.wide = n > CCB_MAX_VERTICES_NARROW || ls_kernel == CCB_LS_WIDE;
   p.threads = DescentThreads(n, p.wide);
@@ -247,11 +249,14 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
       sk.smem_rows = false;
       sk.smem_bytes = SmallKSmem(k, n, pitch, ld, sk.threads, sk.smem_state, false);
       if (!sk.smem_state && kClusterDescent) {
-        // the state spread over a cluster's shared memory instead of streaming from L2 (the batched engine
-        // keeps the L2 form: its buckets are one CTA per slot)
+        // the state spread over a cluster's shared memory instead of streaming from L2, when the population's
+        // clusters fit one wave (the batched engine keeps the L2 form: its buckets are one CTA per slot)
         size_t per_cta = 0;
-        sk.cluster = StreamCluster(k, n, limit - 4096, &per_cta);
-        if (sk.cluster > 0) sk.smem_bytes = per_cta;
+        const int c = StreamCluster(k, n, limit - 4096, &per_cta);
+        if (c > 0 && (long long)pop * c <= dev.sms) {
+          sk.cluster = c;
+          sk.smem_bytes = per_cta;
+        }
       }
     }
     p.small_k = true;
@@ -504,8 +509,9 @@ void Describe(ccb_solver& s) {
   s.description = text;
 }
 
-// CCB_REBUILD_AUTO's choice on the wide path.
-constexpr bool kTensorRebuildByDefault = false;
+// CCB_REBUILD_AUTO's choice on the wide path: the tensor cores (measured at G(65536, 0.02), pop 128: the rebuild
+// phase of a 50-iteration solve takes 83 ms at k = 2 and 125 ms at k = 3, against 412 / 654 ms by popcount).
+constexpr bool kTensorRebuildByDefault = true;
 
 // Whether the solver rebuilds G on the tensor cores: the tiled wide rebuild (int32 G) with n >= 128, chosen
 // explicitly or by CCB_REBUILD_AUTO.
@@ -555,7 +561,7 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->pop = pop;
   s->ld = std::max(32, (g->n + 31) / 32 * 32);
   s->ls_kernel = ls_kernel;
-  s->plan = MakePlan(g->n, g->pitch, k, s->ld, s->kpad, ls_kernel, s->device);
+  s->plan = MakePlan(g->n, g->pitch, k, s->ld, s->kpad, ls_kernel, s->device, pop);
   // k = 2, 3 wide on a sparse graph (average degree <= n / 8): work per move follows the degree, not n
   s->plan.sparse = s->plan.packed_wide && 2.0 * (double)g->edges <= (double)g->n * g->n / 8.0;
 
@@ -974,7 +980,7 @@ struct ccb_batch {
   int max_iterations = 0;
   long long replays = 0;
   double l2_share = 0.0;  // 0: persistent grids fill every SM (see BuildWorkLists)
-  int engine = CCB_BATCH_FLOW;
+  int engine = CCB_BATCH_LOCKSTEP;
   double wait_limit_sec = 30.0;        // flow engine: a block's idle wait gives up after this long
   std::vector<int32_t> withheld;       // per instance: its flow work is never published (fault injection)
   FlowState* d_flow = nullptr;         // per entry
@@ -1515,7 +1521,7 @@ size_t RequestBytes(const ccb_server& sv, uint32_t n, const ccb_params& p) {
   const size_t graph = (size_t)std::max<uint32_t>(n, 1) * pitch * 4 + (size_t)std::max<uint32_t>(n, 1) * 4;
   const int ld = std::max(32, ((int)n + 31) / 32 * 32);
   const int kpad = (p.k + 3) / 4 * 4;
-  const Plan plan = MakePlan((int)n, pitch, p.k, ld, kpad, CCB_LS_AUTO, sv.device);
+  const Plan plan = MakePlan((int)n, pitch, p.k, ld, kpad, CCB_LS_AUTO, sv.device, p.population);
   const size_t labels = (size_t)p.population * ld;
   const size_t gb = plan.wide ? 4 : 2;
   const size_t next = plan.smem_state ? 0
@@ -1597,7 +1603,8 @@ bool BatchedKernelsTake(const ccb_server& sv, const ccb_server::Request& r) {
   const int words = (int)((r.n + 31) / 32);
   const int pitch = std::max(4, (words + 3) / 4 * 4);
   const int ld = std::max(32, ((int)r.n + 31) / 32 * 32);
-  const Plan pl = MakePlan((int)r.n, pitch, r.params.k, ld, (r.params.k + 3) / 4 * 4, CCB_LS_AUTO, sv.device);
+  const Plan pl = MakePlan((int)r.n, pitch, r.params.k, ld, (r.params.k + 3) / 4 * 4, CCB_LS_AUTO, sv.device,
+                           r.params.population);
   return !pl.wide && (pl.small_k || pl.incremental);
 }
 

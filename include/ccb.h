@@ -178,13 +178,15 @@ int ccb_batch_add(ccb_batch* batch, const ccb_graph* graph, const ccb_params* pa
  * is the instance's own completion time from the start of the run under the flow engine, the run's time under
  * the lock-step engine. */
 int ccb_batch_run(ccb_batch* batch);
-/* The engine, chosen before the first run.  CCB_BATCH_FLOW (default): one persistent kernel per shape bucket
- * carries every instance through all its iterations; a block claims the next (instance, slot) item of the
- * heaviest instance that has one, and the block that completes an instance's last descent (rebuild) slot runs
- * its record and stop rule (advances its iteration) and publishes its next phase, so no instance waits for
- * another.  A block that finds nothing to claim while instances are unfinished sleeps, and gives up after
- * wait_limit_sec (0: 30 s) with CCB_ERR_TIMEOUT.  CCB_BATCH_LOCKSTEP: one CUDA graph replay per iteration of
- * all instances. */
+/* The engine, chosen before the first run.  CCB_BATCH_LOCKSTEP (default): one CUDA graph replay per iteration
+ * of all instances (bucket descents, then record, rebuild and advance of every instance).  CCB_BATCH_FLOW: one
+ * persistent kernel per shape bucket carries every instance through all its iterations; a block claims the next
+ * (instance, slot) item of the heaviest instance that has one, and the block that completes an instance's last
+ * descent (rebuild) slot runs its record and stop rule (advances its iteration) and publishes its next phase,
+ * so no instance waits for another: small instances finish early (per-instance completion far sooner) at some
+ * cost in whole-batch throughput.  A flow block that finds nothing to claim while instances are unfinished
+ * sleeps, leaves when its bucket has more blocks than unfinished slots, and gives up after wait_limit_sec
+ * (0: 30 s) with CCB_ERR_TIMEOUT. */
 enum ccb_batch_engine { CCB_BATCH_FLOW = 0, CCB_BATCH_LOCKSTEP = 1 };
 int ccb_batch_set_engine(ccb_batch* batch, int32_t engine, double wait_limit_sec);
 /* Host-side fault injection for tests of the bounded wait: instance `id`'s work is never published to the flow

@@ -86,9 +86,10 @@ def _mix_subset(ccb, iterations):
     return [mix[i] for kind in sorted(kinds) for _, i in sorted(kinds[kind])[:2]]
 
 
-def test_batched_mix_at_100_iterations(ccb, oracle, cuda_device):
+@pytest.mark.parametrize("engine", ["lockstep", "flow"])
+def test_batched_mix_at_100_iterations(ccb, oracle, cuda_device, engine):
     subset = _mix_subset(ccb, 100)
-    batch = ccb.Batch()
+    batch = ccb.Batch(engine=engine)
     runs = []
     for inst in subset:
         dg, _ = ccb.DeviceGraph.planted(inst.n, inst.parts, inst.p_in, inst.p_out, inst.flip, inst.graph_seed)
