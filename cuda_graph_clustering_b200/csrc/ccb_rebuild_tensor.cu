@@ -15,11 +15,12 @@ namespace ccb {
 namespace {
 
 constexpr int kTileK = 128;                         // vertices u per pipeline stage: one 128-byte row
-constexpr int kStages = 4;
+constexpr int kStages = 3;
+constexpr int kSubTiles = 2;                        // 128-row accumulators per CTA, sharing each Z stage
 constexpr int kMmaK = 32;                           // K of one kind::i8 MMA, in bytes
 constexpr int kThreads = 192;                       // warp 0 TMA, warp 1 MMA + TMEM, warps 2..5 expand + epilogue
-constexpr int kATileBytes = kTensorTileM * kTileK;  // int8 A tile per stage: 16 KiB
-constexpr int kBitsTileBytes = kTensorTileM * 16;   // adjacency words per stage: 4 per row, 2 KiB
+constexpr int kATileBytes = kTensorTileM * kTileK;  // int8 A sub-tile per stage: 16 KiB
+constexpr int kBitsTileBytes = kTensorTileM * 16;   // adjacency words of a sub-tile per stage: 4 per row, 2 KiB
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // a wait gives up after 2 s ...
 constexpr uint32_t kWaitSpinLimit = 1u << 24;               // ... or this many polls
 
@@ -171,10 +172,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int bn = a.bn;
-  uint8_t* s_a = base;                                  // [stage][128 rows][128 B], swizzled
-  uint8_t* s_b = s_a + kStages * kATileBytes;           // [stage][bn rows][128 B], swizzled by TMA
-  uint8_t* s_bits = s_b + kStages * bn * kTileK;        // [stage][128 rows][16 B]
-  uint64_t* full = reinterpret_cast<uint64_t*>(s_bits + kStages * kBitsTileBytes);
+  uint8_t* s_a = base;                                        // [stage][sub][128 rows][128 B], swizzled
+  uint8_t* s_b = s_a + kStages * kSubTiles * kATileBytes;     // [stage][bn rows][128 B], swizzled by TMA
+  uint8_t* s_bits = s_b + kStages * bn * kTileK;              // [stage][sub][128 rows][16 B]
+  uint64_t* full = reinterpret_cast<uint64_t*>(s_bits + kStages * kSubTiles * kBitsTileBytes);
   uint64_t* a_ready = full + kStages;
   uint64_t* empty = a_ready + kStages;
   uint64_t* accum = empty + kStages;
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x / kWarp;
   const int lane = threadIdx.x % kWarp;
-  const int m0 = blockIdx.x * kTensorTileM;
+  const int m0 = blockIdx.x * kTensorTileM * kSubTiles;
   const int n0 = blockIdx.y * bn;
   const int ktiles = a.ktiles;
 
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0) {
     if (lane == 0) {
       // TMA producer: stage s holds the adjacency words of K step kt and the Z block's bytes of it.
-      const uint32_t bytes = kBitsTileBytes + bn * kTileK;
+      const uint32_t bytes = kSubTiles * kBitsTileBytes + bn * kTileK;
       int issued = 0;
       for (int kt = 0; kt < ktiles; ++kt) {
         const int s = kt % kStages;
@@ -223,7 +224,11 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         BarArriveExpectTx(&full[s], bytes);
-        TmaLoad2d(s_bits + s * kBitsTileBytes, &bits_map, kt * 4, m0, &full[s]);
+#pragma unroll
+        for (int sub = 0; sub < kSubTiles; ++sub) {  // a box past the last row reads zeros
+          TmaLoad2d(s_bits + (s * kSubTiles + sub) * kBitsTileBytes, &bits_map, kt * 4, m0 + sub * kTensorTileM,
+                    &full[s]);
+        }
         TmaLoad2d(s_b + s * bn * kTileK, &z_map, kt * kTileK, n0, &full[s]);
         issued = kt + 1;
       }
@@ -246,11 +251,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         TcFenceAfter();
-        const uint64_t ad = Sw128Desc(a_base + s * kATileBytes);
         const uint64_t bd = Sw128Desc(b_base + s * bn * kTileK);
 #pragma unroll
-        for (int j = 0; j < kTileK / kMmaK; ++j) {
-          MmaI8(tmem, ad + 2 * j, bd + 2 * j, idesc, (kt > 0 || j > 0) ? 1u : 0u);
+        for (int sub = 0; sub < kSubTiles; ++sub) {  // accumulator `sub` in TMEM columns [sub * bn, (sub + 1) * bn)
+          const uint64_t ad = Sw128Desc(a_base + (s * kSubTiles + sub) * kATileBytes);
+#pragma unroll
+          for (int j = 0; j < kTileK / kMmaK; ++j) {
+            MmaI8(tmem + sub * bn, ad + 2 * j, bd + 2 * j, idesc, (kt > 0 || j > 0) ? 1u : 0u);
+          }
         }
         MmaCommit(&empty[s]);  // the stage is free once these MMAs have read it
       }
@@ -268,18 +276,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) give_up();
         break;
       }
-      const uint4 w = *reinterpret_cast<const uint4*>(s_bits + s * kBitsTileBytes + r * 16);
-      const uint32_t words[4] = {w.x, w.y, w.z, w.w};
-      uint8_t* row = s_a + s * kATileBytes + (r >> 3) * 1024 + (r & 7) * kTileK;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const uint32_t h = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-        uint4 out;
-        out.x = Spread4(h & 0xFu);
-        out.y = Spread4((h >> 4) & 0xFu);
-        out.z = Spread4((h >> 8) & 0xFu);
-        out.w = Spread4(h >> 12);
-        *reinterpret_cast<uint4*>(row + ((q ^ (r & 7)) << 4)) = out;
+      for (int sub = 0; sub < kSubTiles; ++sub) {
+        const int t = s * kSubTiles + sub;
+        const uint4 w = *reinterpret_cast<const uint4*>(s_bits + t * kBitsTileBytes + r * 16);
+        const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+        uint8_t* row = s_a + t * kATileBytes + (r >> 3) * 1024 + (r & 7) * kTileK;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const uint32_t h = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+          uint4 out;
+          out.x = Spread4(h & 0xFu);
+          out.y = Spread4((h >> 4) & 0xFu);
+          out.z = Spread4((h >> 8) & 0xFu);
+          out.w = Spread4(h >> 12);
+          *reinterpret_cast<uint4*>(row + ((q ^ (r & 7)) << 4)) = out;
+        }
       }
       FenceProxyAsyncShared();
       __syncwarp();
@@ -290,37 +302,39 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (!ok && lane == 0) give_up();
     TcFenceAfter();
     const int quarter = warp & 3;
-    const int v = m0 + quarter * kWarp + lane;
-    const uint32_t lane_addr = tmem + (static_cast<uint32_t>(quarter * kWarp) << 16);
     const LabelT* labels = static_cast<const LabelT*>(a.labels);
     const bool write = ok && !*abort;
-    int cur_slot = -1, own = -1, part = 0;
-    auto flush = [&]() {
-      const unsigned total = __reduce_add_sync(kAllLanes, static_cast<unsigned>(part));
-      if (lane == 0 && write && cur_slot >= 0 && total != 0) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(a.intra + cur_slot), static_cast<unsigned long long>(total));
-      }
-    };
-    for (int c0 = 0; c0 < bn; c0 += 16) {
-      uint32_t acc[16];
-      TmemLoad16(lane_addr + c0, acc);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int col = n0 + c0 + i;
-        if (col >= a.columns) break;
-        const int slot = col / a.k;
-        if (slot != cur_slot) {
-          flush();
-          cur_slot = slot;
-          part = 0;
-          own = v < a.n ? static_cast<int>(labels[static_cast<size_t>(slot) * a.label_ld + v]) : -1;
+    for (int sub = 0; sub < kSubTiles; ++sub) {
+      const int v = m0 + sub * kTensorTileM + quarter * kWarp + lane;
+      const uint32_t lane_addr = tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + sub * bn;
+      int cur_slot = -1, own = -1, part = 0;
+      auto flush = [&]() {
+        const unsigned total = __reduce_add_sync(kAllLanes, static_cast<unsigned>(part));
+        if (lane == 0 && write && cur_slot >= 0 && total != 0) {
+          atomicAdd(reinterpret_cast<unsigned long long*>(a.intra + cur_slot), static_cast<unsigned long long>(total));
         }
-        const int val = static_cast<int>(acc[i]);
-        if (write && a.g != nullptr && v < a.n_store) a.g[static_cast<size_t>(col) * a.ld + v] = val;
-        if (own == col - slot * a.k) part += val;
+      };
+      for (int c0 = 0; c0 < bn; c0 += 16) {
+        uint32_t acc[16];
+        TmemLoad16(lane_addr + c0, acc);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int col = n0 + c0 + i;
+          if (col >= a.columns) break;
+          const int slot = col / a.k;
+          if (slot != cur_slot) {
+            flush();
+            cur_slot = slot;
+            part = 0;
+            own = v < a.n ? static_cast<int>(labels[static_cast<size_t>(slot) * a.label_ld + v]) : -1;
+          }
+          const int val = static_cast<int>(acc[i]);
+          if (write && a.g != nullptr && v < a.n_store) a.g[static_cast<size_t>(col) * a.ld + v] = val;
+          if (own == col - slot * a.k) part += val;
+        }
       }
+      flush();
     }
-    flush();
   }
   TcFenceBefore();
   __syncthreads();
@@ -406,7 +420,7 @@ EncodeTiledFn EncodeTiled() {
 }
 
 size_t TensorSmem(int bn) {
-  return 1024 + static_cast<size_t>(kStages) * (kATileBytes + bn * kTileK + kBitsTileBytes) +
+  return 1024 + static_cast<size_t>(kStages) * (kSubTiles * (kATileBytes + kBitsTileBytes) + bn * kTileK) +
          (3 * kStages + 1) * sizeof(uint64_t) + 16;
 }
 
@@ -430,9 +444,9 @@ bool PlanTensorRebuild(TensorRebuild& t, int n, int columns, const char** why) {
   t.bn = ((columns + blocks - 1) / blocks + 15) / 16 * 16;
   t.n_tiles = (columns + t.bn - 1) / t.bn;
   t.z_rows = t.n_tiles * t.bn;
-  t.m_tiles = (n + kTensorTileM - 1) / kTensorTileM;
+  t.m_tiles = (n + kTensorTileM * kSubTiles - 1) / (kTensorTileM * kSubTiles);
   t.tmem_cols = 32;
-  while (t.tmem_cols < t.bn) t.tmem_cols *= 2;
+  while (t.tmem_cols < kSubTiles * t.bn) t.tmem_cols *= 2;
   t.smem = TensorSmem(t.bn);
   return true;
 }

@@ -6,12 +6,13 @@
 // one dense contraction with M = n (vertices v), N = pop*k (slot-cluster columns), K = n (vertices u) and
 // 0/1 operands, exact in int32.  Here:
 //   k_build_z       writes Z as uint8 rows [column][kz] (kz = ceil(ceil(n/32)/4) * 128 bytes, zero past n);
-//   k_rebuild_tensor one CTA per 128-vertex tile of v and block of up to 256 columns: TMA brings the tile's
-//                   adjacency words (2 KiB per 128 u) and the Z block (128-byte swizzle) into a 4-stage
-//                   shared-memory pipeline; four warps expand the bits into int8 rows in the UMMA 128-byte
-//                   swizzled K-major layout; one thread issues tcgen05.mma kind::i8 (M 128, N <= 256, K 32);
-//                   the epilogue reads the accumulator (tcgen05.ld) and writes G and each slot's
-//                   intra-cluster sum sum_v G[s][label_s(v)][v].
+//   k_rebuild_tensor one CTA per 256-vertex tile of v (two 128-row accumulators in TMEM) and block of up to
+//                   256 columns: TMA brings the two sub-tiles' adjacency words (2 KiB each per 128 u) and the Z
+//                   block (128-byte swizzle) into a 3-stage shared-memory pipeline; four warps expand the bits
+//                   into int8 rows in the UMMA 128-byte swizzled K-major layout; one thread issues
+//                   tcgen05.mma kind::i8 (M 128, N <= 256, K 32) for both sub-tiles against the same Z stage, so
+//                   each Z byte crossing from L2 serves 256 rows; the epilogue reads the accumulators
+//                   (tcgen05.ld) and writes G and each slot's intra-cluster sum sum_v G[s][label_s(v)][v].
 // Every mbarrier wait is bounded (time and spins); one that gives up sets *error = kErrorWaitTimeout, the
 // kernel drains its own copies and MMAs, frees its TMEM and returns.  Tensor maps cover this GPU's memory
 // only; no load uses cluster multicast.
@@ -27,7 +28,7 @@
 
 namespace ccb {
 
-constexpr int kTensorTileM = 128;  // vertices v per CTA (one TMEM lane each)
+constexpr int kTensorTileM = 128;  // vertices v per accumulator (one TMEM lane each); a CTA holds two
 constexpr int kTensorMaxN = 256;   // columns per CTA (one MMA's N)
 
 struct TensorRebuild {
@@ -42,8 +43,8 @@ struct TensorRebuild {
   int bn = 0;             // columns per CTA, a multiple of 16, <= 256
   int n_tiles = 0;        // column blocks for `columns`
   int z_rows = 0;         // n_tiles * bn
-  int m_tiles = 0;        // ceil(n / 128)
-  int tmem_cols = 0;      // power of two >= bn (and >= 32)
+  int m_tiles = 0;        // ceil(n / 256)
+  int tmem_cols = 0;      // power of two >= 2 * bn (and >= 32)
   size_t smem = 0;        // dynamic shared memory per CTA
 };
 

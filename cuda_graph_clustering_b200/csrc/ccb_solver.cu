@@ -755,17 +755,46 @@ void PrintPlan(const ccb_solver& s, size_t free_hint) {
               Mebibytes(s.device_bytes).c_str(), Mebibytes(free_hint).c_str());
 }
 
+// The record arguments of the iterations of a solve (Progress::Next's stall / early-stop / time rules and the GWW
+// ranking; cc_pbils.hpp:69-78, cc_pbils_gpu.cu:325-345).
+RecordArgs IterationRecord(const ccb_solver& s, const ccb_params& p, TraceEntry* trace) {
+  RecordArgs r{};
+  r.ld = s.ld;
+  r.n = s.n;
+  r.count = s.pop;
+  r.ctl = s.ctl;
+  r.record_labels = s.record_lab;
+  r.early_stop = p.early_stop;
+  r.copies = (int)(p.gww * s.pop);
+  r.src_map = s.src_map;
+  r.order = s.order;
+  r.trace = trace;
+  r.time_limit_ns = p.time_limit_sec > 0 ? (unsigned long long)(p.time_limit_sec * 1e9) : 0ull;
+  r.f = s.next_f;
+  r.labels = s.next_lab;
+  r.mode = kRecordIteration;
+  return r;
+}
+
+// One PBILS iteration of the plain path on `st`: select + descent, record, GWW + perturbation + rebuild
+// (cc_pbils_gpu.cu:347-387).  Once the record has set the stop flag every later kernel returns at once.
+template <typename GainT>
+void LaunchPlainIteration(ccb_solver& s, const ccb_params& p, RecordArgs r, int it, cudaStream_t st) {
+  const int copies = (int)(p.gww * s.pop);
+  const bool perturb = s.k >= 2 && p.perturbation > 0.0;
+  LaunchDescentStep<GainT>(s, s.pop, s.pop, p.tournament, it, StreamSeed(p.seed, kSelectTag, 0), st);
+  r.iteration = it;
+  LaunchRecord(s, r, st);
+  LaunchRebuild<GainT>(s, s.pop, perturb ? kRebuildPerturb : kRebuildCopy, copies > 0 ? s.src_map : nullptr,
+                       StreamSeed(p.seed, kPerturbTag, 0), it, (float)p.perturbation, 0, true, st);
+}
+
 template <typename GainT>
 void RunPbils(ccb_solver& s, const ccb_params& p, cudaStream_t st, int32_t* labels_out, ccb_result* res) {
   TraceRange trace_range("ccb.pbils");
   const auto started = std::chrono::steady_clock::now();
   const int n = s.n, k = s.k, pop = s.pop;
   const uint64_t init_stream = StreamSeed(p.seed, kInitTag, 0);
-  const uint64_t select_stream = StreamSeed(p.seed, kSelectTag, 0);
-  const uint64_t perturb_stream = StreamSeed(p.seed, kPerturbTag, 0);
-  const int copies = (int)(p.gww * pop);
-  const bool perturb = k >= 2 && p.perturbation > 0.0;
-  const float prob = (float)p.perturbation;
   const bool verbose = p.verbose != 0;
   if (verbose) {
     size_t free_b = 0, total_b = 0;
@@ -785,33 +814,16 @@ void RunPbils(ccb_solver& s, const ccb_params& p, cudaStream_t st, int32_t* labe
   CCB_CUDA(cudaGetLastError());
   LaunchRebuild<GainT>(s, pop, kRebuildInPlace, nullptr, 0, 0, 0.f, 0, false, st);
 
-  RecordArgs r{};
-  r.ld = s.ld;
-  r.n = n;
-  r.count = pop;
-  r.ctl = s.ctl;
-  r.record_labels = s.record_lab;
-  r.early_stop = p.early_stop;
-  r.copies = copies;
-  r.src_map = s.src_map;
-  r.order = s.order;
-  r.trace = verbose ? s.trace : nullptr;
-  r.time_limit_ns = p.time_limit_sec > 0 ? (unsigned long long)(p.time_limit_sec * 1e9) : 0ull;
+  RecordArgs r = IterationRecord(s, p, verbose ? s.trace : nullptr);
   r.f = s.cur_f;
   r.labels = s.cur_lab;
   r.mode = kRecordInitial;
   LaunchRecord(s, r, st);
-  r.f = s.next_f;
-  r.labels = s.next_lab;
-  r.mode = kRecordIteration;
+  r = IterationRecord(s, p, verbose ? s.trace : nullptr);
 
   int chunk = 0;
   for (int it = 0; it < p.iterations; ++it) {
-    LaunchDescentStep<GainT>(s, pop, pop, p.tournament, it, select_stream, st);
-    r.iteration = it;
-    LaunchRecord(s, r, st);
-    LaunchRebuild<GainT>(s, pop, perturb ? kRebuildPerturb : kRebuildCopy, copies > 0 ? s.src_map : nullptr,
-                         perturb_stream, it, prob, 0, true, st);
+    LaunchPlainIteration<GainT>(s, p, r, it, st);
     if ((it + 1) % kPollChunk == 0 && it + 1 < p.iterations) {
       // Poll the stop flag one chunk behind the device: the device always has a chunk queued.
       const int slot = chunk % 2;
@@ -1285,6 +1297,7 @@ void PrepareBatch(ccb_batch& b) {
 }
 
 // Initial population, rebuild and record of one instance (as RunPbils does before its loop).
+template <typename GainT>
 void EnqueueInit(ccb_solver& s, const ccb_params& p, cudaStream_t st) {
   CCB_CUDA(cudaMemsetAsync(s.ctl, 0, sizeof(Control), st));
   k_mark_start<<<1, 1, 0, st>>>(s.ctl);
@@ -1292,7 +1305,7 @@ void EnqueueInit(ccb_solver& s, const ccb_params& p, cudaStream_t st) {
   const int init_grid = (int)std::max<long long>(1, std::min<long long>(CeilDiv(total, kAuxThreads), 4096));
   k_init_labels<<<init_grid, kAuxThreads, 0, st>>>(s.cur_lab, s.pop, s.n, s.ld, s.k, StreamSeed(p.seed, kInitTag, 0));
   CCB_CUDA(cudaGetLastError());
-  LaunchRebuild<int16_t>(s, s.pop, kRebuildInPlace, nullptr, 0, 0, 0.f, 0, false, st);
+  LaunchRebuild<GainT>(s, s.pop, kRebuildInPlace, nullptr, 0, 0, 0.f, 0, false, st);
   RecordArgs r{};
   r.f = s.cur_f;
   r.labels = s.cur_lab;
@@ -1358,7 +1371,7 @@ void RunBatch(ccb_batch& b) {
   const cudaStream_t st = b.stream;
   for (int e = 0; e < (int)b.batched.size(); ++e) {
     ccb_batch::Instance& in = b.inst[b.batched[e]];
-    EnqueueInit(*in.solver, in.params, st);
+    EnqueueInit<int16_t>(*in.solver, in.params, st);
   }
   std::vector<FlowState> states;
   unsigned long long flow_t0 = 0;
@@ -1442,15 +1455,23 @@ struct ccb_server {
     ccb_result result{};
     std::vector<int32_t> labels;
   };
-  // A request the batched kernels do not take (wide, k = 1, ...), solved on the plain path by a host thread
-  // of its own on a stream of its own, so its kernels overlap the batched iterations.
-  struct Side {
+  // A request the batched kernels do not take (wide: n > 32767; k = 1), solved by the plain path's kernels on a
+  // stream of its own that the server loop steps a chunk of iterations at a time, between the lanes' iterations.
+  struct Wide {
     Active a;
     cudaStream_t stream = nullptr;
-    std::thread worker;
-    std::atomic<bool> finished{false};
-    Done out;
+    cudaEvent_t done = nullptr;
+    Control* h_ctl = nullptr;  // pinned: the control block after the last chunk
+    int next = 0;              // first iteration not yet enqueued
+    bool in_flight = false;
+    ~Wide() {
+      if (stream) cudaStreamSynchronize(stream);
+      if (h_ctl) cudaFreeHost(h_ctl);
+      if (done) cudaEventDestroy(done);
+      if (stream) cudaStreamDestroy(stream);
+    }
   };
+  static constexpr int kWideChunk = 4;
   Device device;
   size_t budget = 0;
   int max_active = 0;
@@ -1489,24 +1510,20 @@ struct ccb_server {
   std::unordered_map<int, Done> done;
   cudaStream_t stream = nullptr;  // admission: graph upload or generation, solver initialisation
   long long steps = 0;
-  std::vector<std::unique_ptr<Side>> sides;
-  int max_sides = 4;
+  std::vector<std::unique_ptr<Wide>> wides;
+  int max_wides = 4;
 
   static int LaneOf(uint32_t n) { return n <= 1024 ? 0 : n <= 2048 ? 1 : n <= 4096 ? 2 : n <= 8192 ? 3 : 4; }
   int ActiveCount() const {
-    size_t c = sides.size();
+    size_t c = wides.size();
     for (const Lane& l : lanes) c += l.active.size();
     return (int)c;
   }
 
   ~ccb_server() {
-    for (auto& sd : sides) {
-      if (sd->worker.joinable()) sd->worker.join();
-      if (sd->stream) cudaStreamDestroy(sd->stream);
-    }
-    sides.clear();
-    for (Lane& l : lanes) {
-      if (l.stream) cudaStreamSynchronize(l.stream);
+    wides.clear();
+    for (Lane& L : lanes) {
+      if (L.stream) cudaStreamSynchronize(L.stream);
     }
     if (stream) cudaStreamDestroy(stream);
   }
@@ -1531,62 +1548,102 @@ size_t RequestBytes(const ccb_server& sv, uint32_t n, const ccb_params& p) {
          (size_t)p.population * p.k * pitch * 4 + 2 * (size_t)p.population * 4 + ld + sizeof(Control);
 }
 
-// Starts the plain solve of an admitted request on a worker thread (the request's memory stays charged to
-// the budget until it is collected).
-void StartSide(ccb_server& sv, ccb_server::Active&& a) {
-  std::unique_ptr<ccb_server::Side> sd(new ccb_server::Side());
-  sd->a = std::move(a);
-  CCB_CUDA(cudaStreamCreateWithFlags(&sd->stream, cudaStreamNonBlocking));
-  sv.in_use += sd->a.req.bytes;
-  ccb_server::Side* raw = sd.get();
-  const int device = sv.device.id;
-  raw->worker = std::thread([raw, device] {
-    ccb_server::Done& d = raw->out;
-    try {
-      CCB_CUDA(cudaSetDevice(device));
-      ccb_solver& s = *raw->a.solver;
-      d.labels.resize(s.n);
-      if (s.plan.wide) {
-        RunPbils<int32_t>(s, raw->a.req.params, raw->stream, d.labels.data(), &d.result);
-      } else {
-        RunPbils<int16_t>(s, raw->a.req.params, raw->stream, d.labels.data(), &d.result);
-      }
-    } catch (const Failure& f) {
-      d.status = f.status;
-      d.error = f.message;
-    } catch (const std::bad_alloc&) {
-      d.status = CCB_ERR_DEVICE_MEMORY;
-      d.error = "host allocation failed";
-    } catch (const std::exception& e) {
-      d.status = CCB_ERR_CUDA;
-      d.error = e.what();
-    }
-    raw->finished.store(true, std::memory_order_release);
-  });
-  sv.sides.push_back(std::move(sd));
+// Sets up the plain solve of an admitted request on a stream of its own (its memory stays charged to the budget
+// until it is retired); the server loop then enqueues its iterations a chunk at a time.
+void StartWide(ccb_server& sv, ccb_server::Active&& a) {
+  std::unique_ptr<ccb_server::Wide> w(new ccb_server::Wide());
+  w->a = std::move(a);
+  CCB_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+  CCB_CUDA(cudaEventCreateWithFlags(&w->done, cudaEventDisableTiming));
+  CCB_CUDA(cudaMallocHost(&w->h_ctl, sizeof(Control)));
+  std::memset(w->h_ctl, 0, sizeof(Control));  // read before the first chunk's copy lands: not stopped
+  ccb_solver& s = *w->a.solver;
+  if (s.plan.wide) {
+    EnqueueInit<int32_t>(s, w->a.req.params, w->stream);
+  } else {
+    EnqueueInit<int16_t>(s, w->a.req.params, w->stream);
+  }
+  sv.in_use += w->a.req.bytes;
+  sv.wides.push_back(std::move(w));
 }
 
-// Collects the side solves that finished; appends their ids.
-void CollectSides(ccb_server& sv, std::vector<int>& finished) {
-  for (size_t i = 0; i < sv.sides.size();) {
-    ccb_server::Side& sd = *sv.sides[i];
-    if (!sd.finished.load(std::memory_order_acquire)) {
+// The next chunk of iterations of every idle wide request, each followed by a copy of its control block.
+void LaunchWides(ccb_server& sv) {
+  for (auto& wp : sv.wides) {
+    ccb_server::Wide& w = *wp;
+    if (w.in_flight || w.a.cancel) continue;
+    ccb_solver& s = *w.a.solver;
+    const ccb_params& p = w.a.req.params;
+    const int last = std::min(p.iterations, w.next + ccb_server::kWideChunk);
+    const RecordArgs r = IterationRecord(s, p, nullptr);
+    for (int it = w.next; it < last; ++it) {
+      if (s.plan.wide) {
+        LaunchPlainIteration<int32_t>(s, p, r, it, w.stream);
+      } else {
+        LaunchPlainIteration<int16_t>(s, p, r, it, w.stream);
+      }
+    }
+    w.next = last;
+    CCB_CUDA(cudaMemcpyAsync(w.h_ctl, s.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w.stream));
+    CCB_CUDA(cudaEventRecord(w.done, w.stream));
+    w.in_flight = true;
+  }
+}
+
+// Retires the wide requests whose chunk completed and that stopped (or were cancelled); returns whether any chunk
+// completed.
+bool RetireWides(ccb_server& sv, std::vector<int>& finished) {
+  bool any = false;
+  for (size_t i = 0; i < sv.wides.size();) {
+    ccb_server::Wide& w = *sv.wides[i];
+    if (w.in_flight) {
+      const cudaError_t q = cudaEventQuery(w.done);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      CCB_CUDA(q);
+      w.in_flight = false;
+      any = true;
+    }
+    const ccb_params& p = w.a.req.params;
+    if (!w.a.cancel && !w.h_ctl->stop && w.next < p.iterations) {
       ++i;
       continue;
     }
-    sd.worker.join();
-    cudaStreamDestroy(sd.stream);
-    sd.stream = nullptr;
-    sd.out.result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - sd.a.admitted).count();
-    if (sd.a.cancel) {
-      sd.out.status = CCB_ERR_CANCELLED;
-      sd.out.error = "request cancelled";
+    if (w.a.cancel) {
+      CCB_CUDA(cudaStreamSynchronize(w.stream));
+      ccb_server::Done d;
+      d.status = CCB_ERR_CANCELLED;
+      d.error = "request cancelled";
+      sv.done[w.a.req.id] = std::move(d);
+    } else {
+      ccb_solver& s = *w.a.solver;
+      std::vector<int32_t> labels(s.n);
+      CopyOutLabels(s, labels.data(), w.stream);
+      const Control& c = s.host_ctl[0];
+      ccb_server::Done d;
+      try {
+        CheckDeviceError(c);
+        d.result.objective = c.record_f;
+        d.result.iterations_done = c.iterations_done;
+        d.result.local_searches = (int64_t)c.iterations_done * s.pop;
+        d.result.accepted_moves = (int64_t)c.moves;
+        d.result.clusters_used = CountClustersUsed(labels.data(), (uint32_t)s.n, s.k);
+        d.result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - w.a.admitted).count();
+        d.labels = std::move(labels);
+      } catch (const Failure& f) {
+        d.status = f.status;
+        d.error = f.message;
+      }
+      sv.done[w.a.req.id] = std::move(d);
     }
-    sv.in_use -= sd.a.req.bytes;
-    finished.push_back(sd.a.req.id);
-    sv.done[sd.a.req.id] = std::move(sd.out);
-    sv.sides.erase(sv.sides.begin() + i);
+    finished.push_back(w.a.req.id);
+    sv.in_use -= w.a.req.bytes;
+    sv.wides.erase(sv.wides.begin() + i);
+    any = true;
   }
+  return any;
 }
 
 void Finish(ccb_server& sv, ccb_server::Active& a, const ccb_result& r, std::vector<int32_t> labels) {
@@ -1597,7 +1654,7 @@ void Finish(ccb_server& sv, ccb_server::Active& a, const ccb_result& r, std::vec
   sv.done[a.req.id] = std::move(d);
 }
 
-// Whether a request runs in the batched iterations (else on a side thread): the plan's narrow small-k or
+// Whether a request runs in the batched iterations (else stepped alone on its stream): the plan's narrow small-k or
 // incremental descents.
 bool BatchedKernelsTake(const ccb_server& sv, const ccb_server::Request& r) {
   const int words = (int)((r.n + 31) / 32);
@@ -1616,7 +1673,7 @@ void Admit(ccb_server& sv) {
   while (!sv.queue.empty() && sv.ActiveCount() < sv.max_active) {
     ccb_server::Request& r = sv.queue.front();
     if (sv.in_use + r.bytes > sv.budget && sv.ActiveCount() > 0) break;
-    if ((int)sv.sides.size() >= sv.max_sides && r.n > 0 && !BatchedKernelsTake(sv, r)) break;
+    if ((int)sv.wides.size() >= sv.max_wides && r.n > 0 && !BatchedKernelsTake(sv, r)) break;
     ccb_server::Active a;
     a.admitted = std::chrono::steady_clock::now();
     a.req = std::move(r);
@@ -1646,10 +1703,10 @@ void Admit(ccb_server& sv) {
       const Plan& pl = a.solver->plan;
       if (pl.wide || !(pl.small_k || pl.incremental)) {
         CCB_CUDA(cudaStreamSynchronize(sv.stream));  // the graph is complete before another stream reads it
-        StartSide(sv, std::move(a));
+        StartWide(sv, std::move(a));
         continue;
       }
-      EnqueueInit(*a.solver, q.params, sv.stream);
+      EnqueueInit<int16_t>(*a.solver, q.params, sv.stream);
     } catch (const Failure& f) {
       // the request fails alone (its graph or buffers could not be made): ccb_server_result reports the error
       ccb_server::Done d;
@@ -1751,7 +1808,7 @@ void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t
   std::vector<int> before_ids;
   before_ids.reserve(sv.done.size());
   for (const auto& kv : sv.done) before_ids.push_back(kv.first);
-  CollectSides(sv, newly);
+  RetireWides(sv, newly);
   Admit(sv);
   if (sv.done.size() != done_before + newly.size()) {
     std::sort(before_ids.begin(), before_ids.end());
@@ -1765,8 +1822,11 @@ void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t
     if (!L.in_flight && !L.active.empty()) LaunchLane(L, sv.device);
     any |= L.in_flight;
   }
+  LaunchWides(sv);
+  for (const auto& w : sv.wides) any |= w->in_flight;
   if (any) {
-    // wait until at least one lane finished its iteration (bounded: every kernel of an iteration ends)
+    // wait until at least one lane finished its iteration or one wide request its chunk (bounded: every kernel
+    // of an iteration ends)
     for (bool got = false; !got;) {
       for (ccb_server::Lane& L : sv.lanes) {
         if (!L.in_flight) continue;
@@ -1776,11 +1836,10 @@ void ServerStep(ccb_server& sv, int32_t* finished_ids, int32_t capacity, int32_t
         RetireLane(sv, L, newly);
         got = true;
       }
+      got |= RetireWides(sv, newly);
       if (!got) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
     ++sv.steps;
-  } else if (!sv.sides.empty()) {
-    std::this_thread::sleep_for(std::chrono::microseconds(200));
   }
   if (finished_count) *finished_count = (int32_t)newly.size();
   if (finished_ids) {
@@ -2111,8 +2170,8 @@ int ccb_server_cancel(ccb_server* sv, int32_t id, int32_t* found) {
         if (!hit && a.req.id == id && !a.cancel) a.cancel = hit = true;
       }
     }
-    for (auto& sd : sv->sides) {
-      if (!hit && sd->a.req.id == id && !sd->a.cancel) sd->a.cancel = hit = true;
+    for (auto& w : sv->wides) {
+      if (!hit && w->a.req.id == id && !w->a.cancel) w->a.cancel = hit = true;
     }
     if (found) *found = hit;
   });

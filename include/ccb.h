@@ -226,10 +226,11 @@ int ccb_tuning_get(ccb_tuning_entry* entries, int32_t capacity, int32_t* count);
  * Admitted requests run in five lanes by size (n <= 1024, 2048, 4096, 8192, larger), each stepping one PBILS
  * iteration of all its requests at a time on a stream of its own, so the lanes overlap on the device and a
  * small request is not held to the pace of a large one; requests admitted later join their lane at its next
- * iteration.  A step launches every idle lane, waits until at least one lane finished its iteration, and
- * retires the requests that stopped, freeing their memory for the queue.  Each result equals the request's
- * plain solve.  Requests the batched kernels do not take (k = 1, n > 32767) run their plain solve on a host
- * thread of their own, overlapping the lanes.  Not thread-safe: one host thread drives a server. */
+ * iteration.  Requests the batched kernels do not take (k = 1, n > 32767) are stepped by the same loop on a stream
+ * of their own each, four iterations of the plain path's kernels at a time, so their kernels overlap the lanes'
+ * on the device.  A step launches every idle lane and wide request, waits until at least one of them finished
+ * its iteration (chunk), and retires the requests that stopped, freeing their memory for the queue.  Each
+ * result equals the request's plain solve.  Not thread-safe: one host thread drives a server. */
 typedef struct ccb_server ccb_server;
 /* hbm_budget_bytes 0: 80% of the free device memory; max_active 0: 1024. */
 int ccb_server_create(uint64_t hbm_budget_bytes, int32_t max_active, ccb_server** out);
@@ -248,8 +249,8 @@ int ccb_server_status(const ccb_server* server, int32_t* queued, int32_t* active
 /* done = 1 and the result (labels: n int32) once request `id` finished; the result is then released. */
 int ccb_server_result(ccb_server* server, int32_t id, int32_t* done, int32_t* labels_out, ccb_result* result);
 /* Cancels request `id` (found = 0 if it is unknown or already finished): a queued request leaves the queue, an
- * admitted one stops before its lane's next iteration and frees its memory when that iteration completes, a
- * request on a side thread runs to its end and is then dropped.  Its result reports CCB_ERR_CANCELLED. */
+ * admitted one stops before its next iteration (chunk) and frees its memory when the one in flight completes.
+ * Its result reports CCB_ERR_CANCELLED. */
 int ccb_server_cancel(ccb_server* server, int32_t id, int32_t* found);
 void ccb_server_destroy(ccb_server* server);
 

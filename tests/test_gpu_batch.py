@@ -182,7 +182,7 @@ def test_server_same_alone_and_in_the_mix(ccb, cuda_device):
         sv.close()
     sv = ccb.Server(hbm_budget_bytes=3 << 20, max_active=4)
     ids = [sv.submit(host, p) for host, p in reqs]
-    # device-generated requests beside the host ones: one batched, one beyond the narrow limit (side thread)
+    # device-generated requests beside the host ones: one batched, one beyond the narrow limit (stepped on its own stream)
     gp = ccb.PbilsParams(k=6, population=16, iterations=5, early_stop=3, seed=12)
     gid = sv.submit_generated(gp, 900, planted=True, parts=3, p_in=0.6, p_out=0.1, flip=0.05, seed=77)
     wp = ccb.PbilsParams(k=5, population=4, iterations=2, early_stop=3, seed=13)
@@ -250,4 +250,30 @@ def test_server_cancel_queued_and_admitted(ccb, cuda_device):
         sv.result(ids[2])
     assert queued.value.status == ccb._native.CCB_ERR_CANCELLED
     assert _results_equal(results[ids[1]], ccb.SolveGpu(host, ps[1]))
+    sv.close()
+
+
+def test_server_steps_wide_requests_and_cancels_one(ccb, cuda_device):
+    """Requests beyond the narrow limit are stepped by the server loop, a chunk of iterations at a time on their
+    own streams, beside a batched lane: each finishes with its plain solve's result, and one cancelled while its
+    chunk runs reports CCB_ERR_CANCELLED without disturbing the others."""
+    sv = ccb.Server()
+    wp = ccb.PbilsParams(k=3, population=8, iterations=12, early_stop=12, seed=5)
+    a = sv.submit_generated(wp, 36000, density=0.003, seed=90)
+    b = sv.submit_generated(wp, 40000, density=0.003, seed=91)
+    np_ = ccb.PbilsParams(k=6, population=16, iterations=6, early_stop=6, seed=6)
+    c = sv.submit_generated(np_, 1200, planted=True, parts=3, p_in=0.6, p_out=0.1, flip=0.05, seed=92)
+    sv.step()  # all three admitted: two wide chunks and one lane iteration in flight
+    assert sv.cancel(b)
+    results, errors = {}, {}
+    while len(results) + len(errors) < 3:
+        for i in sv.step():
+            try:
+                results[i] = sv.result(i)
+            except ccb.CcbError as e:
+                errors[i] = e
+    assert errors[b].status == ccb._native.CCB_ERR_CANCELLED
+    assert _results_equal(results[a], ccb.SolveGpu(ccb.DeviceGraph.erdos_renyi(36000, 0.003, 90).download(), wp))
+    dg, _ = ccb.DeviceGraph.planted(1200, 3, 0.6, 0.1, 0.05, 92)
+    assert _results_equal(results[c], ccb.SolveGpu(dg.download(), np_))
     sv.close()
