@@ -154,15 +154,26 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.txt), or None."""
+def profiled_value(name: str, key: str):
+    """A `key: value` figure from a committed summary under profiles/ (name without .txt), or None."""
     path = os.path.join(REPO, "profiles", name + ".txt")
     try:
         with open(path) as fh:
-            m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", fh.read())
+            m = re.search(re.escape(key) + r":\s*([0-9.eE+]+)", fh.read())
             return float(m.group(1)) if m else None
     except OSError:
         return None
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.txt), or None."""
+    return profiled_value(name, "dram_bytes_per_launch")
+
+
+def measured_peaks():
+    """L2 copy GB/s and int8 tensor TOPS measured on this pool (profiles/peaks_l2_hbm_int8.txt, written by
+    cuda_graph_clustering_b200/peaks.py)."""
+    return profiled_value("peaks_l2_hbm_int8", "l2_copy_gbs"), profiled_value("peaks_l2_hbm_int8", "int8_tops")
 
 
 def reference_cpu_run(cfg, iterations, threads=0):
@@ -577,6 +588,21 @@ def run_neighborhood(args, rank, world, local):
         per_move = n * (2 * 2 + 1) + 4 * words + 8 * deg  # SURVEY 8(d) generic move bytes at k = 2, sG = 2
         modelled = moves_per_launch * per_move / (descent_ms * 1e-3) / 1e9
         peak, peak_kind = measured_peak_hbm()
+        # the register descent (k = 2, 1024 threads x 4 vertices): issue roofline with the instructions per move
+        # of its own ncu summary (profiles/k_descent_neighborhood.txt), the modelled bytes beside
+        inst_per_move = profiled_value("k_descent_neighborhood", "warp_inst_per_move_per_block")
+        sm_hz = (clock_info.get("sm_mhz") or 1965.0) * 1e6
+        issue_peak = torch.cuda.get_device_properties(local).multi_processor_count * 4 * sm_hz / 1e9
+        ach = (inst_per_move or 0.0) * moves_per_launch / (descent_ms * 1e-3) / 1e9
+        nb_roofline = {"bound": "issue", "achieved": ach if inst_per_move else None, "peak": issue_peak,
+                       "unit": "G warp-inst/s", "frac": ach / issue_peak if inst_per_move else None,
+                       "traffic": profiled_traffic("k_descent_neighborhood"), "kernel": "k_descent_registers",
+                       "avg_launch_ms": descent_ms,
+                       "limiter": "latency of the per-move chain; instructions per move from "
+                                  "profiles/k_descent_neighborhood.txt",
+                       "modelled_bytes": {"achieved_gbs": modelled, "hbm_peak_gbs": peak, "hbm_peak_kind": peak_kind,
+                                          "frac_of_hbm": modelled / peak,
+                                          "per_move": "n(2k+1) + 4 ceil(n/32) + 8 deg (SURVEY 8(d))"}}
         cpu = None
         if not args.no_cpu_baseline:
             sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -605,11 +631,7 @@ def run_neighborhood(args, rank, world, local):
             "objective": results[True][0].objective,
             "e2e": {"value": moves_all / t_e2e, "unit": "moves/s", "h2d_bytes_per_step": int(graph.bits.nbytes),
                     "d2h_bytes_per_step": int(4 * n + 48), "bit_exact": bool(e2e_ok)},
-            "roofline": {"bound": "alu", "kernel": "k_descent", "avg_launch_ms": descent_ms,
-                         "note": "state in registers and shared memory; see the plain workload's ALU-pipe profile",
-                         "modelled_bytes": {"achieved_gbs": modelled, "hbm_peak_gbs": peak, "peak_kind": peak_kind,
-                                            "frac": modelled / peak,
-                                            "per_move": "n(2k+1) + 4 ceil(n/32) + 8 deg (SURVEY 8(d))"}},
+            "roofline": nb_roofline,
             "kernel_ms_per_solve": {"descent": st.descent_ms, "rebuild": st.rebuild_ms, "record": st.record_ms,
                                     "other": st.other_ms},
             # per step pair: the solve with the local search, and the one without (no descent launches)
@@ -775,6 +797,38 @@ def main():
         peak, peak_kind = measured_peak_hbm()
         achieved = per_launch / (descent_ms * 1e-3) / 1e9
         traffic = profiled_traffic(f"k_descent_{args.workload}")
+        l2_peak, int8_peak = measured_peaks()
+        modelled = {"achieved_gbs": achieved, "hbm_peak_gbs": peak, "hbm_peak_kind": peak_kind,
+                    "frac_of_hbm": achieved / peak, "bytes_per_launch": per_launch,
+                    "basis": "SURVEY 8(d) algorithmic bytes per accepted move (a modelled rate: the state is "
+                             "read from registers, shared memory or L2)"}
+        plan = solver.describe()
+        if "registers" in plan and "incremental" not in plan:
+            # the register descent: bound by the latency of its per-move chain, seen as issue utilisation
+            inst_per_move = profiled_value("k_descent_plain", "warp_inst_per_move_per_block")
+            sm_hz = (clock_info.get("sm_mhz") or 1965.0) * 1e6
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            issue_peak = sms * 4 * sm_hz / 1e9
+            ach = (inst_per_move or 0.0) * moves_per_launch / (descent_ms * 1e-3) / 1e9
+            roofline = {"bound": "issue", "achieved": ach, "peak": issue_peak, "unit": "G warp-inst/s",
+                        "frac": ach / issue_peak, "traffic": traffic, "kernel": "k_descent_registers",
+                        "avg_launch_ms": descent_ms,
+                        "limiter": "latency of the per-move chain (row word, scan, warp minimum, block barrier); "
+                                   "instructions per move from profiles/k_descent_plain.txt",
+                        "peak_kind": "issue slots of all SMs (4 per SM per cycle) at the sampled SM clock",
+                        "modelled_bytes": modelled}
+        elif "L2" in plan and l2_peak:
+            roofline = {"bound": "l2", "achieved": achieved, "peak": l2_peak, "unit": "GB/s",
+                        "frac": achieved / l2_peak, "traffic": traffic, "kernel": "k_descent",
+                        "avg_launch_ms": descent_ms, "peak_kind": "measured L2 copy (profiles/peaks_l2_hbm_int8.txt)",
+                        "basis": modelled["basis"], "modelled_bytes": modelled}
+        else:
+            roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_descent",
+                        "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": descent_ms}
+        if rebuild_compare is not None and int8_peak:
+            rebuild_compare["int8_peak_tops"] = int8_peak
+            rebuild_compare["tensor_phase_frac_of_int8_peak"] = rebuild_compare["tensor_phase_tops"] / int8_peak
         value = iters_all / (total_ms_all * 1e-3)
         cpu = None
         have_ref = os.path.exists(os.path.join(REPO, "oracle", "_ref", "cc_cpu"))
@@ -818,10 +872,7 @@ def main():
             "e2e": {"value": iters_all / e2e_all, "unit": "iter/s",
                     "h2d_bytes_per_step": int(graph.bits.nbytes), "d2h_bytes_per_step": int(4 * n + 48),
                     "bit_exact": e2e_ok},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_descent", "algorithmic_bytes_per_launch": per_launch,
-                         "avg_launch_ms": descent_ms},
+            "roofline": roofline,
             "kernel_ms_per_solve": {"descent": st.descent_ms, "rebuild": st.rebuild_ms, "record": st.record_ms,
                                     "other": st.other_ms},
             "gpu_launches": int(launches_per_solve * args.steps),

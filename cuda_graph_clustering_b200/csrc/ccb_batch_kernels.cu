@@ -173,11 +173,19 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
         idle_since = 0;
       } else if (LoadAcquire(b.remaining) <= 0 || LoadAcquire(b.error) != 0) {
         s_flag = 1;  // the bucket is done (or gave up): leave
-      } else if (LoadAcquire(b.remaining + 2) > LoadAcquire(b.remaining + 1)) {
-        // more blocks run than the unfinished instances have slots: this one is never needed again, and its SM is
-        // freed for the other buckets
-        s_flag = 1;
       } else {
+        // more blocks run than the unfinished instances have slots: a surplus block is never needed again and
+        // leaves, freeing its SM for the other buckets.  The decision is taken on the count after this block's
+        // own decrement, so blocks that look at the same time cannot all leave: as many stay as there are slots
+        if (LoadAcquire(b.remaining + 2) > LoadAcquire(b.remaining + 1)) {
+          if (atomicSub(b.remaining + 2, 1) - 1 >= LoadAcquire(b.remaining + 1)) {
+            s_flag = 2;  // left (already counted out)
+          } else {
+            atomicAdd(b.remaining + 2, 1);  // still needed: stay
+          }
+        }
+      }
+      if (s_entry < 0 && s_flag == 0) {
         const unsigned long long now = GlobalTimerNs();
         if (idle_since == 0) {
           idle_since = now;
@@ -191,7 +199,7 @@ __device__ __forceinline__ void FlowLoop(const BatchEntry* __restrict__ entries,
     __syncthreads();
     if (s_entry < 0) {
       if (s_flag) {
-        if (threadIdx.x == 0) atomicSub(b.remaining + 2, 1);
+        if (threadIdx.x == 0 && s_flag == 1) atomicSub(b.remaining + 2, 1);
         break;
       }
       continue;

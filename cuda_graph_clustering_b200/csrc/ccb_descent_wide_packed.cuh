@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "ccb_device.cuh"
 #include "ccb_streams.cuh"
@@ -240,8 +241,8 @@ struct WideBest2 {
 // cluster.  Keys: cluster 0 max of (e + 2^20) << 11 | (2047 - j), cluster 1 min of (e + 2^20) << 11 | j, with
 // j = 32 i + lane the vertex's place among the owner's (lower j = lower vertex); e > -2^20 keeps both
 // sentinels (0 and ~0) out of reach.
-template <int W>
-__device__ __forceinline__ void WarpRescanWide2(const int32_t* state, int n, int words, int owner_word0, int owner,
+template <int W, typename StateT>
+__device__ __forceinline__ void WarpRescanWide2(const StateT* state, int n, int words, int owner_word0, int owner,
                                                 WideBest2& b) {
   const int lane = threadIdx.x % kWarp;
   uint32_t k0 = 0u, k1 = ~0u;
@@ -277,10 +278,15 @@ __device__ __forceinline__ void WarpRescanWide2(const int32_t* state, int n, int
   }
 }
 
-template <int T, int W>
+// kSmem16: the slot's words 2e + label as int16 in shared memory (n * 2 bytes), exact while every degree is below
+// 16384 (|2e + label| <= 2 deg + 1 < 2^15); else int32 in the slot's rows of `next` (global memory, L2).  Every
+// thread reads and writes only its own vertices' words, so the two placements run the same code.
+template <int T, int W, bool kSmem16>
 __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a, int slot) {
   using Key = unsigned long long;
+  using StateT = typename std::conditional<kSmem16, int16_t, int32_t>::type;
   constexpr int kWarps = T / kWarp;
+  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
   __shared__ int s_stop;
   __shared__ MoveRecord<Key> s_records[2 * kWarps];
@@ -308,7 +314,8 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
   if (s_stop) return;
   const int w = s_winner;
 
-  int32_t* state = a.next.g + static_cast<size_t>(slot) * a.k * ld;
+  StateT* state = kSmem16 ? reinterpret_cast<StateT*>(smem)
+                          : reinterpret_cast<StateT*>(a.next.g + static_cast<size_t>(slot) * a.k * ld);
   WideBest2 b;
   b.Clear();
   {
@@ -319,7 +326,7 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
 #pragma unroll 1
     for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
       const int u = 32 * q + lane;
-      if (u < n) state[u] = 2 * (g[ld + u] - g[u]) + lab[u];
+      if (u < n) state[u] = static_cast<StateT>(2 * (g[ld + u] - g[u]) + lab[u]);
     }
     __syncwarp();
 #pragma unroll 1
@@ -395,7 +402,7 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
         for (int c = 0; c < 4; ++c) {
           if (us[c] < 0) continue;
           const int wd = ws[c] + step;
-          state[us[c]] = wd;
+          state[us[c]] = static_cast<StateT>(wd);
           if ((wd & 1) == worse) {
             rescan |= us[c] == ((wd & 1) ? b.u1 : b.u0);
           } else {
@@ -409,7 +416,7 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
     const int qv = v >> 5;
     if (qv >= warp * kWarp * W && qv < (warp + 1) * kWarp * W && (qv - warp * kWarp * W) % kWarp == lane) {
       const int wd = state[v] ^ 1;
-      state[v] = wd;
+      state[v] = static_cast<StateT>(wd);
       rescan |= v == (to == 1 ? b.u0 : b.u1);
       b.Offer(wd, v);
     }
@@ -438,9 +445,9 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
   }
 }
 
-template <int T, int W>
+template <int T, int W, bool kSmem16>
 __global__ void __launch_bounds__(T, 1) k_descent_wide2_sparse(DescentArgs<int32_t> a) {
-  DescentWide2Sparse<T, W>(a, blockIdx.x);
+  DescentWide2Sparse<T, W, kSmem16>(a, blockIdx.x);
 }
 
 // k = 3 in the same degree-proportional form.  For a vertex in cluster a the gain of target c is

@@ -44,7 +44,11 @@ cudaError_t LaunchDescentIncrementalWide(const DescentArgs<int32_t>& args, int g
 // vertex in the slot's rows of `next`, no dynamic shared memory.
 // With `sparse`: the degree-proportional forms (per-thread best vertex of each cluster, k = 2, or of each
 // (cluster, target) class, k = 3).
-cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& args, int grid, bool sparse, cudaStream_t stream);
+// With `smem16` (k = 2 sparse only): the slot's words as int16 in shared memory (Wide2Smem16Bytes(n) bytes), for
+// graphs whose degrees are all below 16384.
+cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& args, int grid, bool sparse, bool smem16,
+                                    cudaStream_t stream);
+size_t Wide2Smem16Bytes(int n);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);
 

@@ -167,6 +167,7 @@ struct Plan {
   bool incremental = false; // the incremental 9 <= k <= 64 descent
   bool packed_wide = false;  // the packed wide descent (k = 2, 3)
   bool sparse = false;       // k = 2 packed wide: the degree-proportional form (sparse graphs)
+  bool smem16 = false;       // k = 2 sparse: the slot's words as int16 in shared memory (every degree < 16384)
   SmallKPlan sk;
 };
 
@@ -355,6 +356,8 @@ const char* KernelName(const Plan& p) {
       return p.sparse ? "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), L2"
                       : "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2";
     }
+    if (p.smem16) return "packed wide k = 2, degree-proportional (per-thread best of each cluster), int16 state in "
+                         "shared memory";
     return p.sparse ? "packed wide k = 2, degree-proportional (per-thread best of each cluster), L2"
                     : "packed wide k = 2 (e = G1 - G0 and the label, 4 bytes per vertex), L2";
   }
@@ -500,6 +503,22 @@ struct ccb_solver {
 
 namespace {
 
+// The largest vertex degree of a device graph (a host copy of its degree array).
+int MaxDegree(const ccb_graph& g) {
+  std::vector<int32_t> d(std::max(g.n, 1));
+  if (g.n > 0) CCB_CUDA(cudaMemcpy(d.data(), g.degrees, (size_t)g.n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return g.n > 0 ? *std::max_element(d.begin(), d.end()) : 0;
+}
+
+// The k = 2 sparse wide descent keeps the slot's words (2e + label) as int16 in shared memory when every degree is
+// below 16384 (|2e + 1| < 2^15) and n * 2 bytes fit; else as int32 in global memory.
+void PlanSmem16(ccb_solver& s) {
+  s.plan.smem16 = false;
+  if (!(s.plan.packed_wide && s.plan.sparse && s.k == 2)) return;
+  if (Wide2Smem16Bytes(s.n) + 4096 > (size_t)s.device.smem_optin) return;
+  s.plan.smem16 = MaxDegree(*s.graph) < 16384;
+}
+
 // The plan in words (ccb_solver_describe, --verbose); redone whenever the plan changes.
 void Describe(ccb_solver& s) {
   char text[320];
@@ -564,6 +583,7 @@ ccb_solver* MakeSolver(const ccb_graph* g, int k, int pop, int ls_kernel) {
   s->plan = MakePlan(g->n, g->pitch, k, s->ld, s->kpad, ls_kernel, s->device, pop);
   // k = 2, 3 wide on a sparse graph (average degree <= n / 8): work per move follows the degree, not n
   s->plan.sparse = s->plan.packed_wide && 2.0 * (double)g->edges <= (double)g->n * g->n / 8.0;
+  PlanSmem16(*s);
 
   const size_t labels = (size_t)pop * s->ld;
   const size_t gains = labels * k;
@@ -721,7 +741,7 @@ void LaunchDescentStep(ccb_solver& s, int grid, int population, int tournament, 
   } else {
     if (s.plan.packed_wide) {
       cudaError_t e = cudaSuccess;
-      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentWidePacked(a, grid, s.plan.sparse, st); });
+      s.timer.Time(kCatDescent, st, [&] { e = LaunchDescentWidePacked(a, grid, s.plan.sparse, s.plan.smem16, st); });
       CCB_CUDA(e);
       return;
     }
@@ -1360,6 +1380,9 @@ unsigned long long RunFlow(ccb_batch& b, std::vector<FlowState>& states) {
   if (error == kErrorWaitTimeout) {
     Fail(CCB_ERR_TIMEOUT, "batched flow engine: a block found no work to claim for the wait limit (" +
                               std::to_string(b.wait_limit_sec) + " s) while instances were unfinished");
+  }
+  for (int e = 0; e < count; ++e) {
+    if (!states[e].finished) Fail(CCB_ERR_STATE, "batched flow engine: the run ended with an unfinished instance");
   }
   return t0;
 }
@@ -2216,6 +2239,7 @@ ccb_solver& CachedSolver(const uint32_t* bits, uint32_t n, uint32_t words_per_ro
     // the plan's k = 2 / 3 wide form depends on the density
     ccb_solver& s = *c.solver;
     s.plan.sparse = s.plan.packed_wide && 2.0 * (double)edges <= (double)n * n / 8.0;
+    PlanSmem16(s);
     Describe(s);
     return s;
   }
