@@ -36,30 +36,45 @@ cudaError_t Wide2Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st
   return cudaErrorInvalidValue;  // a shared-memory state this large does not fit
 }
 
+template <int W, bool kSmem24>
+cudaError_t GoWide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st) {
+  auto kernel = k_descent_wide3_sparse<1024, W, kSmem24>;
+  size_t smem = 0;
+  if (kSmem24) {
+    smem = Wide3Smem24Bytes(a.gr.n);
+    const cudaError_t e = RaiseDynamicSmem(kernel, smem);
+    if (e != cudaSuccess) return e;
+  }
+  if (grid > 0) kernel<<<grid, 1024, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <bool kSmem24>
+cudaError_t Wide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st) {
+  const int words = (a.gr.n + 31) / 32;
+  const int per_thread = (words + 1023) / 1024;
+  if (per_thread <= 1) return GoWide3Sparse<1, kSmem24>(a, grid, st);
+  if (per_thread <= 2) return GoWide3Sparse<2, kSmem24>(a, grid, st);
+  if (per_thread <= 4) return GoWide3Sparse<4, kSmem24>(a, grid, st);
+  if constexpr (!kSmem24) {
+    if (per_thread <= 8) return GoWide3Sparse<8, false>(a, grid, st);
+    if (per_thread <= 16) return GoWide3Sparse<16, false>(a, grid, st);
+    return GoWide3Sparse<32, false>(a, grid, st);
+  }
+  return cudaErrorInvalidValue;  // a shared-memory state this large does not fit
+}
+
 }  // namespace
 
 size_t Wide2Smem16Bytes(int n) { return ((size_t)n * 2 + 15) / 16 * 16; }
+size_t Wide3Smem24Bytes(int n) { return ((size_t)n * 3 + 15) / 16 * 16 + 16; }
 
 cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& a, int grid, bool sparse, bool smem16,
                                     cudaStream_t st) {
   if (a.k == 2 && sparse) {
     return smem16 ? Wide2Sparse<true>(a, grid, st) : Wide2Sparse<false>(a, grid, st);
   } else if (a.k == 3 && sparse) {
-    const int words = (a.gr.n + 31) / 32;
-    const int per_thread = (words + 1023) / 1024;
-    if (per_thread <= 1) {
-      k_descent_wide3_sparse<1024, 1><<<grid, 1024, 0, st>>>(a);
-    } else if (per_thread <= 2) {
-      k_descent_wide3_sparse<1024, 2><<<grid, 1024, 0, st>>>(a);
-    } else if (per_thread <= 4) {
-      k_descent_wide3_sparse<1024, 4><<<grid, 1024, 0, st>>>(a);
-    } else if (per_thread <= 8) {
-      k_descent_wide3_sparse<1024, 8><<<grid, 1024, 0, st>>>(a);
-    } else if (per_thread <= 16) {
-      k_descent_wide3_sparse<1024, 16><<<grid, 1024, 0, st>>>(a);
-    } else {
-      k_descent_wide3_sparse<1024, 32><<<grid, 1024, 0, st>>>(a);
-    }
+    return smem16 ? Wide3Sparse<true>(a, grid, st) : Wide3Sparse<false>(a, grid, st);
   } else if (a.k == 2) {
     k_descent_wide_packed<2, 1024><<<grid, 1024, 0, st>>>(a);
   } else if (a.k == 3) {

@@ -481,16 +481,53 @@ __device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, ui
   }
 }
 
-template <int W>
-__device__ __forceinline__ void WarpRescanWide3(const unsigned long long* state, int n, int words, int owner_word0,
-                                                int owner, uint32_t (&key)[6]) {
+// Where a k = 3 slot keeps its vertex words.  Wide3Global: the 64-bit words (three 20-bit counters + label) in
+// the slot's rows of `next` (global memory, L2).  Wide3Smem24: a 24-bit record per vertex in shared memory (G1 and
+// G2 in 11 bits each, the label in 2; G0 = degree - G1 - G2), exact while every degree is below 2048; the record
+// of vertex u sits at byte 3u, so the 32 vertices of a row word q fill the 24 words [24q, 24q + 24) and every
+// thread writes only words of its own.  Both present the same 64-bit word to the descent.
+struct Wide3Global {
+  unsigned long long* p;
+  __device__ __forceinline__ unsigned long long Load(int u) const { return p[u]; }
+  __device__ __forceinline__ void Store(int u, unsigned long long w) const { p[u] = w; }
+};
+
+struct Wide3Smem24 {
+  uint32_t* words;
+  const int32_t* degrees;
+  __device__ __forceinline__ unsigned long long Load(int u) const {
+    const int o = 3 * u;
+    const int wi = o >> 2, sh = (o & 3) * 8;
+    uint32_t rec = words[wi] >> sh;
+    if (sh >= 16) rec |= words[wi + 1] << (32 - sh);
+    rec &= 0xFFFFFFu;
+    const unsigned long long g1 = rec & 2047u, g2 = (rec >> 11) & 2047u, label = rec >> 22;
+    const unsigned long long g0 = static_cast<unsigned long long>(degrees[u]) - g1 - g2;
+    return g0 | g1 << 20 | g2 << 40 | label << 60;
+  }
+  __device__ __forceinline__ void Store(int u, unsigned long long w) const {
+    const uint32_t rec = static_cast<uint32_t>((w >> 20) & 2047u) | static_cast<uint32_t>((w >> 40) & 2047u) << 11 |
+                         static_cast<uint32_t>(w >> 60) << 22;
+    const int o = 3 * u;
+    const int wi = o >> 2, sh = (o & 3) * 8;
+    words[wi] = (words[wi] & ~(0xFFFFFFu << sh)) | (rec << sh);
+    if (sh >= 16) {
+      const uint32_t hi_mask = 0xFFFFFFu >> (32 - sh);
+      words[wi + 1] = (words[wi + 1] & ~hi_mask) | (rec >> (32 - sh));
+    }
+  }
+};
+
+template <int W, typename State>
+__device__ __forceinline__ void WarpRescanWide3(const State& state, int n, int words, int owner_word0, int owner,
+                                                uint32_t (&key)[6]) {
   const int lane = threadIdx.x % kWarp;
   uint32_t k[6] = {0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll(W < 8 ? W : 8)
   for (int i = 0; i < W; ++i) {
     const int q = owner_word0 + i * kWarp;
     const int u = 32 * q + lane;
-    if (q < words && u < n) Wide3Offer(state[u], static_cast<uint32_t>(i * kWarp + lane), k);
+    if (q < words && u < n) Wide3Offer(state.Load(u), static_cast<uint32_t>(i * kWarp + lane), k);
   }
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
@@ -499,11 +536,13 @@ __device__ __forceinline__ void WarpRescanWide3(const unsigned long long* state,
   }
 }
 
-template <int T, int W>
+template <int T, int W, bool kSmem24>
 __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a, int slot) {
   using Key = unsigned long long;
   using Word = unsigned long long;
+  using State = typename std::conditional<kSmem24, Wide3Smem24, Wide3Global>::type;
   constexpr int kWarps = T / kWarp;
+  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
   __shared__ int s_stop;
   __shared__ MoveRecord<Key> s_records[2 * kWarps];
@@ -532,17 +571,41 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
   if (s_stop) return;
   const int w = s_winner;
 
-  Word* state = reinterpret_cast<Word*>(a.next.g + static_cast<size_t>(slot) * a.k * ld);
+  State state;
+  if constexpr (kSmem24) {
+    state = State{reinterpret_cast<uint32_t*>(smem), a.gr.degrees};
+  } else {
+    state = State{reinterpret_cast<Word*>(a.next.g + static_cast<size_t>(slot) * a.k * ld)};
+  }
   uint32_t key[6] = {0u, 0u, 0u, 0u, 0u, 0u};
   {
     const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
     const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
+    if constexpr (kSmem24) {
+      // a thread writes the vertices of its own row words only (the 24-bit records of a word's 32 vertices share
+      // memory words with nothing else): the vertices of word q = word0 + 32 i are written by this thread
 #pragma unroll 1
-    for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
-      const int u = 32 * q + lane;
-      if (u < n) {
-        state[u] = static_cast<Word>(g[u]) | static_cast<Word>(g[ld + u]) << 20 |
-                   static_cast<Word>(g[2 * ld + u]) << 40 | static_cast<Word>(lab[u]) << 60;
+      for (int i = 0; i < W; ++i) {
+        const int q = word0 + i * kWarp;
+        if (q >= words) continue;
+#pragma unroll 1
+        for (int b = 0; b < 32; ++b) {
+          const int u = 32 * q + b;
+          if (u < n) {
+            state.Store(u, static_cast<Word>(g[u]) | static_cast<Word>(g[ld + u]) << 20 |
+                               static_cast<Word>(g[2 * ld + u]) << 40 | static_cast<Word>(lab[u]) << 60);
+          }
+        }
+      }
+    } else {
+      // the warp builds its owners' words 32 at a time (vertex 32 q + lane of each of its words q)
+#pragma unroll 1
+      for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+        const int u = 32 * q + lane;
+        if (u < n) {
+          state.Store(u, static_cast<Word>(g[u]) | static_cast<Word>(g[ld + u]) << 20 |
+                             static_cast<Word>(g[2 * ld + u]) << 40 | static_cast<Word>(lab[u]) << 60);
+        }
       }
     }
     __syncwarp();
@@ -608,12 +671,12 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
           }
         }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : Word{};
+        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state.Load(us[c]) : Word{};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           if (us[c] < 0) continue;
           const Word wd = ws[c] + step;
-          state[us[c]] = wd;
+          state.Store(us[c], wd);
           const int au = static_cast<int>(wd >> 60);
           const uint32_t j = static_cast<uint32_t>(i * kWarp + (us[c] & 31));
           const int ga = Wide3G(wd, au);
@@ -635,9 +698,9 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
     // v changes cluster (its counters are unchanged: no self-loops)
     const int qv = v >> 5;
     if (qv >= warp_word0 && qv < warp_word0 + kWarp * W && (qv - warp_word0) % kWarp == lane) {
-      const Word old = state[v];
+      const Word old = state.Load(v);
       const Word wd = (old & ((static_cast<Word>(1) << 60) - 1)) | static_cast<Word>(to) << 60;
-      state[v] = wd;
+      state.Store(v, wd);
       const uint32_t j = static_cast<uint32_t>(((qv - warp_word0) / kWarp) * kWarp + (v & 31));
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
@@ -659,7 +722,7 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
 #pragma unroll 1
   for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
     const int u = 32 * q + lane;
-    if (u < n) dst[u] = static_cast<uint8_t>(state[u] >> 60);
+    if (u < n) dst[u] = static_cast<uint8_t>(state.Load(u) >> 60);
   }
   if (tid == 0) {
     a.next.f[slot] = objective;
@@ -667,9 +730,9 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
   }
 }
 
-template <int T, int W>
+template <int T, int W, bool kSmem24>
 __global__ void __launch_bounds__(T, 1) k_descent_wide3_sparse(DescentArgs<int32_t> a) {
-  DescentWide3Sparse<T, W>(a, blockIdx.x);
+  DescentWide3Sparse<T, W, kSmem24>(a, blockIdx.x);
 }
 
 }  // namespace ccb

@@ -167,7 +167,7 @@ struct Plan {
   bool incremental = false; // the incremental 9 <= k <= 64 descent
   bool packed_wide = false;  // the packed wide descent (k = 2, 3)
   bool sparse = false;       // k = 2 packed wide: the degree-proportional form (sparse graphs)
-  bool smem16 = false;       // k = 2 sparse: the slot's words as int16 in shared memory (every degree < 16384)
+  bool smem16 = false;       // sparse k = 2 / 3: the slot's words in shared memory (int16 / 24-bit records)
   SmallKPlan sk;
 };
 
@@ -353,6 +353,8 @@ void LaunchDescent(const Plan& p, const DescentArgs<GainT>& a, int grid, cudaStr
 const char* KernelName(const Plan& p) {
   if (p.packed_wide) {
     if (p.sk.k == 3) {
+      if (p.smem16) return "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), "
+                           "24-bit records in shared memory";
       return p.sparse ? "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), L2"
                       : "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2";
     }
@@ -510,13 +512,15 @@ int MaxDegree(const ccb_graph& g) {
   return g.n > 0 ? *std::max_element(d.begin(), d.end()) : 0;
 }
 
-// The k = 2 sparse wide descent keeps the slot's words (2e + label) as int16 in shared memory when every degree is
-// below 16384 (|2e + 1| < 2^15) and n * 2 bytes fit; else as int32 in global memory.
+// The sparse wide descents keep the slot's words in shared memory when they fit: k = 2 as int16 (2e + label) when
+// every degree is below 16384 (|2e + 1| < 2^15), k = 3 as 24-bit records (two 11-bit counters and the label) when
+// every degree is below 2048; else in global memory (int32 / 64-bit words).
 void PlanSmem16(ccb_solver& s) {
   s.plan.smem16 = false;
-  if (!(s.plan.packed_wide && s.plan.sparse && s.k == 2)) return;
-  if (Wide2Smem16Bytes(s.n) + 4096 > (size_t)s.device.smem_optin) return;
-  s.plan.smem16 = MaxDegree(*s.graph) < 16384;
+  if (!(s.plan.packed_wide && s.plan.sparse && (s.k == 2 || s.k == 3))) return;
+  const size_t bytes = s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem24Bytes(s.n);
+  if (bytes + 4096 > (size_t)s.device.smem_optin) return;
+  s.plan.smem16 = MaxDegree(*s.graph) < (s.k == 2 ? 16384 : 2048);
 }
 
 // The plan in words (ccb_solver_describe, --verbose); redone whenever the plan changes.
