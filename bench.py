@@ -146,12 +146,18 @@ class ClockSampler:
 
 
 def measured_peak_hbm():
+    """HBM copy GB/s: the pool's MEASURED_PEAKS.json when present, else this repository's own measurement on the
+    same B200s (profiles/peaks_l2_hbm_int8.txt), else the 6650 GB/s recipe fallback."""
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
         with open(path) as fh:
             return float(json.load(fh)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
-        return 6650.0, "fallback"
+        pass
+    own = profiled_value("peaks_l2_hbm_int8", "hbm_copy_gbs")
+    if own:
+        return own, "measured (profiles/peaks_l2_hbm_int8.txt)"
+    return 6650.0, "fallback"
 
 
 def profiled_value(name: str, key: str):
@@ -822,6 +828,17 @@ def main():
                         "frac": achieved / l2_peak, "traffic": traffic, "kernel": "k_descent",
                         "avg_launch_ms": descent_ms, "peak_kind": "measured L2 copy (profiles/peaks_l2_hbm_int8.txt)",
                         "basis": modelled["basis"], "modelled_bytes": modelled}
+        elif "degree-proportional" in plan:
+            # the sparse wide descents: per move one bitset row and the moved vertex's neighbours, a dependent
+            # chain (block argmin -> row load -> neighbour updates -> owner warp's rescan) whose latency, not
+            # bandwidth, sets the pace; the modelled bytes against HBM show how far from a memory bound it runs
+            roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_descent_wide_sparse",
+                        "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": descent_ms,
+                        "limiter": "latency of the per-move chain (block argmin, bitset row, neighbour updates, "
+                                   "rescan); the slot's state "
+                                   + ("in shared memory" if " in shared memory," in plan else "in L2"),
+                        "ns_per_move_per_slot": descent_ms * 1e6 / max(moves_per_launch / pop, 1.0)}
         else:
             roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_descent",
