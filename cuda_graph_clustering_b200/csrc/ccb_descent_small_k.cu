@@ -11,9 +11,9 @@
 namespace ccb {
 namespace {
 
-template <int K, int T, bool S>
+template <int K, int T, bool S, bool H = false>
 cudaError_t GoStream(const DescentArgs<int16_t>& a, int grid, size_t smem, cudaStream_t st, bool configure) {
-  auto kernel = k_descent_stream<K, T, S>;
+  auto kernel = k_descent_stream<K, T, S, H>;
   if (configure) return RaiseDynamicSmem(kernel, smem);
   kernel<<<grid, T, smem, st>>>(a);
   return cudaGetLastError();
@@ -69,11 +69,13 @@ cudaError_t ByPlacement(const SmallKPlan& p, const DescentArgs<int16_t>& a, int 
     }
   }
   if (p.threads == 512) {
-    return p.smem_state ? GoStream<K, 512, true>(a, grid, p.smem_bytes, st, cfg)
-                        : GoStream<K, 512, false>(a, grid, p.smem_bytes, st, cfg);
+    if (p.smem_state) return GoStream<K, 512, true>(a, grid, p.smem_bytes, st, cfg);
+    return p.l2_hints ? GoStream<K, 512, false, true>(a, grid, p.smem_bytes, st, cfg)
+                      : GoStream<K, 512, false>(a, grid, p.smem_bytes, st, cfg);
   }
-  return p.smem_state ? GoStream<K, 1024, true>(a, grid, p.smem_bytes, st, cfg)
-                      : GoStream<K, 1024, false>(a, grid, p.smem_bytes, st, cfg);
+  if (p.smem_state) return GoStream<K, 1024, true>(a, grid, p.smem_bytes, st, cfg);
+  return p.l2_hints ? GoStream<K, 1024, false, true>(a, grid, p.smem_bytes, st, cfg)
+                    : GoStream<K, 1024, false>(a, grid, p.smem_bytes, st, cfg);
 }
 
 template <int T, bool S>

@@ -42,4 +42,48 @@ struct PackedGains<8> {
 
 constexpr int PackedLanes(int k) { return k <= 2 ? 2 : (k <= 4 ? 4 : 8); }
 
+// L2 eviction priorities for state that streams from global memory (PTX createpolicy + .L2::cache_hint): the
+// slots' packed vectors are re-read every move and should stay in L2 (evict_last), while bitset rows are read
+// once per move at random and should leave first (evict_first).  Hints only: the values read and written are
+// the same as with plain accesses.  The accesses are volatile so that a load is never hoisted out of the move
+// loop or merged with the same address's load of another move.
+__device__ __forceinline__ uint64_t L2PolicyEvictLast() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t L2PolicyEvictFirst() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t LoadL2Hint(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint2 LoadL2Hint(const uint2* a, uint64_t pol) {
+  uint2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(a), "l"(pol)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ uint4 LoadL2Hint(const uint4* a, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ void StoreL2Hint(uint32_t* a, uint32_t v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" :: "l"(a), "r"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void StoreL2Hint(uint2* a, uint2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.u32 [%0], {%1, %2}, %3;" :: "l"(a), "r"(v.x), "r"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void StoreL2Hint(uint4* a, uint4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;"
+               :: "l"(a), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "l"(pol) : "memory");
+}
+
 }  // namespace ccb

@@ -11,6 +11,9 @@
 // lanes to / from of every neighbour (no carries: G_from >= 1 there, and lanes stay below 2^16), moves
 // the bias of v from lane `from` to lane `to`, and changes off[from], off[to] by -16 / +16.  The update is
 // folded into the next scan; vertices are taken four at a time with their loads issued first.
+// With the state in global memory and kHint, its accesses carry an L2 evict_last priority and the bitset rows
+// evict_first: the population's packed state (128 slots x 32000 vertices x 16 bytes = 64 MB) then stays in L2
+// while the rows (128 MB at n = 32000) stream past it, instead of the rows evicting dirty state lines.
 #pragma once
 
 #include <cstdint>
@@ -51,8 +54,9 @@ __device__ __forceinline__ void ShiftLane(typename PackedGains<KP>::Vec& v, int 
   PackedGains<KP>::Add(v, d);
 }
 
-template <int K, int T, bool kSmemState>
+template <int K, int T, bool kSmemState, bool kHint = false>
 __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int slot) {
+  static_assert(!(kSmemState && kHint), "L2 hints are for state in global memory");
   constexpr int KP = PackedLanes(K);
   constexpr int U = 4;  // vertices in flight per thread
   using P = PackedGains<KP>;
@@ -85,6 +89,25 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
   const int w = s_winner;
 
   Vec* gv = kSmemState ? reinterpret_cast<Vec*>(smem) : reinterpret_cast<Vec*>(a.next.g) + static_cast<size_t>(slot) * ld;
+  [[maybe_unused]] uint64_t keep = 0, drop = 0;
+  if constexpr (kHint) {
+    keep = L2PolicyEvictLast();
+    drop = L2PolicyEvictFirst();
+  }
+  auto load = [&](int u) -> Vec {
+    if constexpr (kHint) {
+      return LoadL2Hint(gv + u, keep);
+    } else {
+      return gv[u];
+    }
+  };
+  auto store = [&](int u, const Vec& x) {
+    if constexpr (kHint) {
+      StoreL2Hint(gv + u, x, keep);
+    } else {
+      gv[u] = x;
+    }
+  };
   int off[K];
   {
     const int16_t* g_src = a.cur.g + static_cast<size_t>(w) * K * ld;
@@ -110,7 +133,7 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
       } else {
         v = make_uint4(words[0], words[1], words[2], words[3]);
       }
-      gv[u] = v;
+      store(u, v);
     }
   }
   long long objective = a.cur.f[w];
@@ -136,8 +159,12 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
       for (int i = 0; i < U; ++i) {
         const int u = base + i * T;
         if (u < n) {
-          v[i] = gv[u];
-          rw[i] = prev_row != nullptr ? prev_row[u >> 5] : 0u;
+          v[i] = load(u);
+          if constexpr (kHint) {
+            rw[i] = prev_row != nullptr ? LoadL2Hint(prev_row + (u >> 5), drop) : 0u;
+          } else {
+            rw[i] = prev_row != nullptr ? prev_row[u >> 5] : 0u;
+          }
         } else {
           rw[i] = 0u;
         }
@@ -148,7 +175,7 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
         if (u < n) {
           if (rw[i] & lane_bit) {
             P::Add(v[i], delta);
-            gv[u] = v[i];
+            store(u, v[i]);
           }
           int keys[K];
           LaneKeys<K, KP, 0>::Run(v[i], off, keys);
@@ -178,10 +205,10 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
       delta[i] = ((to >> 1) == i ? (1u << (16 * (to & 1))) : 0u) - ((from >> 1) == i ? (1u << (16 * (from & 1))) : 0u);
     }
     if (v % T == tid) {
-      Vec x = gv[v];
+      Vec x = load(v);
       ShiftLane<KP>(x, from, 0xFFFF8000u);  // the own-cluster bias leaves lane `from` (no borrow: bit 15 set)
       ShiftLane<KP>(x, to, 0x8000u);        // and enters lane `to` (no carry: G_to < 2^15)
-      gv[v] = x;
+      store(v, x);
     }
     prev_row = a.gr.bits + static_cast<size_t>(v) * pitch;
     objective += MoveDelta(m.key, bits);
@@ -194,7 +221,12 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
 
   uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
   for (int u = tid; u < n; u += T) {
-    const Vec x = gv[u];
+    Vec x;
+    if constexpr (kHint) {
+      x = LoadL2Hint(gv + u, drop);  // the last read of this launch: the line may leave first now
+    } else {
+      x = gv[u];
+    }
     int own = 0;
 #pragma unroll
     for (int c = 0; c < K; ++c) {
@@ -210,9 +242,9 @@ __device__ __forceinline__ void DescentStream(const DescentArgs<int16_t>& a, int
 }
 
 // One slot per block (plain path).
-template <int K, int T, bool kSmemState>
+template <int K, int T, bool kSmemState, bool kHint>
 __global__ void __launch_bounds__(T, 1) k_descent_stream(DescentArgs<int16_t> a) {
-  DescentStream<K, T, kSmemState>(a, blockIdx.x);
+  DescentStream<K, T, kSmemState, kHint>(a, blockIdx.x);
 }
 
 }  // namespace ccb

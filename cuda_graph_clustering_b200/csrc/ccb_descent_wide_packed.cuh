@@ -377,39 +377,49 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
     const int worse = to;  // e up hurts cluster 1 (smallest e wanted), e down hurts cluster 0
     const uint32_t* row = a.gr.bits + static_cast<size_t>(v) * pitch;
     bool rescan = false;
-#pragma unroll(W < 4 ? W : 4)
-    for (int i = 0; i < W; ++i) {
-      const int q = word0 + i * kWarp;
-      uint32_t mbits = q < words ? row[q] : 0u;
-      const int base = 32 * (word0 + i * kWarp);
-      while (mbits) {
-        // up to four neighbours with their loads in flight together
-        int us[4];
-        int ws[4];
-        int cnt = 0;
+    constexpr int kChunk = W < 4 ? W : 4;  // row words in flight together (one memory latency per chunk)
+#pragma unroll 1
+    for (int i0 = 0; i0 < W; i0 += kChunk) {
+      uint32_t rwords[kChunk];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          us[c] = -1;
-          if (mbits) {
-            us[c] = base + __ffs(mbits) - 1;
-            mbits &= mbits - 1;
-            ++cnt;
+      for (int t = 0; t < kChunk; ++t) {
+        const int q = word0 + (i0 + t) * kWarp;
+        rwords[t] = q < words ? row[q] : 0u;
+      }
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t) {
+        const int i = i0 + t;
+        uint32_t mbits = rwords[t];
+        const int base = 32 * (word0 + i * kWarp);
+        while (mbits) {
+          // up to four neighbours with their loads in flight together
+          int us[4];
+          int ws[4];
+          int cnt = 0;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            us[c] = -1;
+            if (mbits) {
+              us[c] = base + __ffs(mbits) - 1;
+              mbits &= mbits - 1;
+              ++cnt;
+            }
           }
-        }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : 0;
+          for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : 0;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (us[c] < 0) continue;
-          const int wd = ws[c] + step;
-          state[us[c]] = static_cast<StateT>(wd);
-          if ((wd & 1) == worse) {
-            rescan |= us[c] == ((wd & 1) ? b.u1 : b.u0);
-          } else {
-            b.Offer(wd, us[c]);
+          for (int c = 0; c < 4; ++c) {
+            if (us[c] < 0) continue;
+            const int wd = ws[c] + step;
+            state[us[c]] = static_cast<StateT>(wd);
+            if ((wd & 1) == worse) {
+              rescan |= us[c] == ((wd & 1) ? b.u1 : b.u0);
+            } else {
+              b.Offer(wd, us[c]);
+            }
           }
+          (void)cnt;
         }
-        (void)cnt;
       }
     }
     // v itself changes cluster (its e is unchanged: no self-loops)
@@ -457,8 +467,8 @@ __global__ void __launch_bounds__(T, 1) k_descent_wide2_sparse(DescentArgs<int32
 // smallest (gain, vertex, target) over the six.  A move of v from f to t changes d of every neighbour in class
 // (a, c) by [c = t] - [c = f] - [a = t] + [a = f], the same for all of them: better (a compare), worse (a
 // rescan if the class's best is among them) or unchanged; v leaves the classes of f and joins those of t.
-// Vertex words as in WidePacked<3>.
-__device__ __forceinline__ int Wide3Class(int a, int c) { return 2 * a + (c > a ? c - 1 : c); }
+// Vertex words as in WidePacked<3>.  Class (a, c) is 2a + (c > a ? c - 1 : c): a's two classes are 2a (its lower
+// foreign target) and 2a + 1 (the higher).
 __device__ __forceinline__ int Wide3Target(int cls) {
   const int a = cls >> 1, r = cls & 1;
   return r < a ? r : r + 1;
@@ -467,17 +477,28 @@ __device__ __forceinline__ int Wide3G(unsigned long long w, int c) {
   return static_cast<int>((w >> (20 * c)) & ((1u << 20) - 1));
 }
 
-// Folds vertex word wd (place j) into the keys of its two classes.
-__device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, uint32_t (&key)[6]) {
+// The keys of vertex word wd (place j) in its two classes: (a, lower foreign target) = class 2a and (a, higher
+// foreign target) = class 2a + 1.
+struct Wide3Keys {
+  int a;
+  uint32_t lo, hi;
+};
+__device__ __forceinline__ Wide3Keys Wide3KeysOf(unsigned long long wd, uint32_t j) {
   const int a = static_cast<int>(wd >> 60);
   const int ga = Wide3G(wd, a);
+  const int clo = a == 0 ? 1 : 0, chi = a == 2 ? 1 : 2;
+  const uint32_t tail = 2047u - j;
+  return Wide3Keys{a, static_cast<uint32_t>(Wide3G(wd, clo) - ga + (1 << 20)) << 11 | tail,
+                   static_cast<uint32_t>(Wide3G(wd, chi) - ga + (1 << 20)) << 11 | tail};
+}
+
+// Folds vertex word wd (place j) into the keys of its two classes.  The six keys are indexed by compile-time
+// class only (a predicate per class) so that they stay in registers.
+__device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, uint32_t (&key)[6]) {
+  const Wide3Keys kk = Wide3KeysOf(wd, j);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (c == a) continue;
-    const uint32_t d = static_cast<uint32_t>(Wide3G(wd, c) - ga + (1 << 20));
-    const uint32_t k = d << 11 | (2047u - j);
-    const int cls = Wide3Class(a, c);
-    key[cls] = max(key[cls], k);
+  for (int cls = 0; cls < 6; ++cls) {
+    if ((cls >> 1) == kk.a) key[cls] = max(key[cls], (cls & 1) ? kk.hi : kk.lo);
   }
 }
 
@@ -644,8 +665,8 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
     const int v = MoveVertex(m.key, bits);
     const int from = static_cast<int>(m.payload & 0xff);
     const int to = static_cast<int>(m.payload >> 8);
-    sz[from] -= 1;
-    sz[to] += 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sz[c] += (c == to) - (c == from);  // compile-time indices: sz stays in registers
     objective += MoveDelta(m.key, bits);
     ++applied;
     if (static_cast<long long>(applied) > move_budget) {
@@ -655,41 +676,52 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
     const Word step = (static_cast<Word>(1) << (20 * to)) - (static_cast<Word>(1) << (20 * from));
     const uint32_t* row = a.gr.bits + static_cast<size_t>(v) * pitch;
     bool rescan = false;
-#pragma unroll(W < 4 ? W : 4)
-    for (int i = 0; i < W; ++i) {
-      const int q = word0 + i * kWarp;
-      uint32_t mbits = q < words ? row[q] : 0u;
-      while (mbits) {
-        int us[4];
-        Word ws[4];
+    constexpr int kChunk = W < 4 ? W : 4;  // row words in flight together (one memory latency per chunk)
+#pragma unroll 1
+    for (int i0 = 0; i0 < W; i0 += kChunk) {
+      uint32_t rwords[kChunk];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          us[c] = -1;
-          if (mbits) {
-            us[c] = 32 * q + __ffs(mbits) - 1;
-            mbits &= mbits - 1;
+      for (int t = 0; t < kChunk; ++t) {
+        const int q = word0 + (i0 + t) * kWarp;
+        rwords[t] = q < words ? row[q] : 0u;
+      }
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t) {
+        const int i = i0 + t;
+        const int q = word0 + i * kWarp;
+        uint32_t mbits = rwords[t];
+        while (mbits) {
+          int us[4];
+          Word ws[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            us[c] = -1;
+            if (mbits) {
+              us[c] = 32 * q + __ffs(mbits) - 1;
+              mbits &= mbits - 1;
+            }
           }
-        }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state.Load(us[c]) : Word{};
+          for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state.Load(us[c]) : Word{};
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (us[c] < 0) continue;
-          const Word wd = ws[c] + step;
-          state.Store(us[c], wd);
-          const int au = static_cast<int>(wd >> 60);
-          const uint32_t j = static_cast<uint32_t>(i * kWarp + (us[c] & 31));
-          const int ga = Wide3G(wd, au);
+          for (int c = 0; c < 4; ++c) {
+            if (us[c] < 0) continue;
+            const Word wd = ws[c] + step;
+            state.Store(us[c], wd);
+            const uint32_t j = static_cast<uint32_t>(i * kWarp + (us[c] & 31));
+            const Wide3Keys kk = Wide3KeysOf(wd, j);
+            const int au = kk.a;
+            const int own = (au == from) - (au == to);
 #pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            if (cc == au) continue;
-            const int delta = (cc == to) - (cc == from) - (au == to) + (au == from);
-            const int cls = Wide3Class(au, cc);
-            const uint32_t k = static_cast<uint32_t>(Wide3G(wd, cc) - ga + (1 << 20)) << 11 | (2047u - j);
-            if (delta > 0) {
-              key[cls] = max(key[cls], k);
-            } else if (delta < 0) {
-              rescan |= (key[cls] & 2047u) == (2047u - j);  // the class's best got worse
+            for (int cls = 0; cls < 6; ++cls) {
+              if ((cls >> 1) != au) continue;
+              const int cc = (cls & 1) ? (au == 2 ? 1 : 2) : (au == 0 ? 1 : 0);
+              const int delta = (cc == to) - (cc == from) + own;
+              if (delta > 0) {
+                key[cls] = max(key[cls], (cls & 1) ? kk.hi : kk.lo);
+              } else if (delta < 0) {
+                rescan |= (key[cls] & 2047u) == (2047u - j);  // the class's best got worse
+              }
             }
           }
         }
@@ -703,8 +735,8 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
       state.Store(v, wd);
       const uint32_t j = static_cast<uint32_t>(((qv - warp_word0) / kWarp) * kWarp + (v & 31));
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        if (cc != from) rescan |= (key[Wide3Class(from, cc)] & 2047u) == (2047u - j) && key[Wide3Class(from, cc)];
+      for (int cls = 0; cls < 6; ++cls) {  // v leaves the two classes of `from`
+        if ((cls >> 1) == from) rescan |= (key[cls] & 2047u) == (2047u - j) && key[cls];
       }
       Wide3Offer(wd, j, key);
     }

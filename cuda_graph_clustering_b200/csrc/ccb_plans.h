@@ -19,6 +19,7 @@ struct SmallKPlan {
   bool smem_rows = false;   // whole bitset in shared memory
   size_t smem_bytes = 0;
   int cluster = 0;          // streamed form whose state does not fit one CTA: CTAs of the cluster holding it
+  bool l2_hints = false;    // streamed form from global memory: state loads/stores evict_last, rows evict_first
 };
 // The smallest cluster (2, 4 or 8 CTAs) whose shares of the packed state fit `limit` bytes of shared memory per
 // CTA, with its bytes per CTA; 0 if none.

@@ -208,6 +208,13 @@ size_t DescentSmem(const Plan& p, int n, int pitch, int k, int ld, int kpad) {
 }
 
 constexpr int kMaxVerticesIncrementalWide = 65536;
+
+// The streamed K <= 8 descent from global memory gives its state an L2 evict_last priority and the bitset rows
+// evict_first; CCB_L2_HINTS=0 launches the plain-access form instead (for comparisons).
+bool StreamL2Hints() {
+  const char* env = std::getenv("CCB_L2_HINTS");
+  return !(env != nullptr && env[0] == '0');
+}
 // The streamed K <= 8 descent with its state in a thread-block cluster's shared memory when it does not fit one
 // CTA, used when all the population's clusters run at once: a slot then moves ~1.8x faster than streaming its
 // state from L2, but takes C SMs instead of one, so with more slots than one wave of clusters the L2 form is
@@ -259,6 +266,7 @@ Plan MakePlan(int n, int pitch, int k, int ld, int kpad, int ls_kernel, const De
           sk.smem_bytes = per_cta;
         }
       }
+      sk.l2_hints = !sk.smem_state && sk.cluster == 0 && StreamL2Hints();
     }
     p.small_k = true;
     p.smem_state = sk.smem_state;
@@ -375,7 +383,9 @@ const char* KernelName(const Plan& p) {
     if (p.sk.registers) return p.smem_rows ? "packed k <= 8, registers, bitset in shared memory"
                                            : "packed k <= 8, registers";
     if (p.sk.cluster > 0) return "packed k <= 8, state in the distributed shared memory of a CTA cluster";
-    return p.smem_state ? "packed k <= 8, streamed from shared memory" : "packed k <= 8, streamed from L2";
+    if (p.smem_state) return "packed k <= 8, streamed from shared memory";
+    return p.sk.l2_hints ? "packed k <= 8, streamed from L2 (state evict_last, rows evict_first)"
+                         : "packed k <= 8, streamed from L2";
   }
   if (p.wide) return "generic wide (int32 G), global memory";
   if (p.smem_state) return p.smem_rows ? "generic, shared memory, bitset in shared memory" : "generic, shared memory";
@@ -526,8 +536,10 @@ void PlanSmem16(ccb_solver& s) {
 // The plan in words (ccb_solver_describe, --verbose); redone whenever the plan changes.
 void Describe(ccb_solver& s) {
   char text[320];
+  // the sparse wide descents size their own shared state at launch (the slot's words when they fit)
+  const size_t smem = s.plan.smem16 ? (s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem24Bytes(s.n)) : s.plan.smem_bytes;
   std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory%s",
-                KernelName(s.plan), s.plan.threads, s.pop * std::max(1, s.plan.sk.cluster), s.plan.smem_bytes,
+                KernelName(s.plan), s.plan.threads, s.pop * std::max(1, s.plan.sk.cluster), smem,
                 s.tensor ? "; G rebuilt on the tensor cores (int8 tcgen05, TMA)" : "");
   s.description = text;
 }
