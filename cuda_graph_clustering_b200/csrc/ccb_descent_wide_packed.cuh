@@ -386,23 +386,25 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
         const int q = word0 + (i0 + t) * kWarp;
         rwords[t] = q < words ? row[q] : 0u;
       }
+      // two row words at a time as one 64-bit mask (word i in the low half, word i + 1 in the high half): a
+      // thread holds about one neighbour per pair at p = 0.02, so one batch of four usually covers both words
 #pragma unroll
-      for (int t = 0; t < kChunk; ++t) {
+      for (int t = 0; t < kChunk; t += 2) {
         const int i = i0 + t;
-        uint32_t mbits = rwords[t];
+        unsigned long long mbits = rwords[t];
+        if (t + 1 < kChunk) mbits |= static_cast<unsigned long long>(rwords[t + 1]) << 32;
         const int base = 32 * (word0 + i * kWarp);
         while (mbits) {
           // up to four neighbours with their loads in flight together
           int us[4];
           int ws[4];
-          int cnt = 0;
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             us[c] = -1;
             if (mbits) {
-              us[c] = base + __ffs(mbits) - 1;
+              const int bit = __ffsll(mbits) - 1;
+              us[c] = base + (bit >> 5) * (32 * kWarp) + (bit & 31);
               mbits &= mbits - 1;
-              ++cnt;
             }
           }
 #pragma unroll
@@ -418,7 +420,6 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
               b.Offer(wd, us[c]);
             }
           }
-          (void)cnt;
         }
       }
     }
@@ -685,19 +686,25 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
         const int q = word0 + (i0 + t) * kWarp;
         rwords[t] = q < words ? row[q] : 0u;
       }
+      // two row words at a time as one 64-bit mask (word i low, word i + 1 high), as in the k = 2 form
 #pragma unroll
-      for (int t = 0; t < kChunk; ++t) {
+      for (int t = 0; t < kChunk; t += 2) {
         const int i = i0 + t;
-        const int q = word0 + i * kWarp;
-        uint32_t mbits = rwords[t];
+        unsigned long long mbits = rwords[t];
+        if (t + 1 < kChunk) mbits |= static_cast<unsigned long long>(rwords[t + 1]) << 32;
+        const int base = 32 * (word0 + i * kWarp);
         while (mbits) {
           int us[4];
+          uint32_t js[4];  // the vertex's place among the thread's: (word index) * 32 + bit
           Word ws[4];
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             us[c] = -1;
+            js[c] = 0u;
             if (mbits) {
-              us[c] = 32 * q + __ffs(mbits) - 1;
+              const int bit = __ffsll(mbits) - 1;
+              us[c] = base + (bit >> 5) * (32 * kWarp) + (bit & 31);
+              js[c] = static_cast<uint32_t>((i + (bit >> 5)) * kWarp + (bit & 31));
               mbits &= mbits - 1;
             }
           }
@@ -708,7 +715,7 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
             if (us[c] < 0) continue;
             const Word wd = ws[c] + step;
             state.Store(us[c], wd);
-            const uint32_t j = static_cast<uint32_t>(i * kWarp + (us[c] & 31));
+            const uint32_t j = js[c];
             const Wide3Keys kk = Wide3KeysOf(wd, j);
             const int au = kk.a;
             const int own = (au == from) - (au == to);
