@@ -829,14 +829,15 @@ def main():
                         "avg_launch_ms": descent_ms, "peak_kind": "measured L2 copy (profiles/peaks_l2_hbm_int8.txt)",
                         "basis": modelled["basis"], "modelled_bytes": modelled}
         elif "degree-proportional" in plan:
-            # the sparse wide descents: per move one bitset row and the moved vertex's neighbours, a dependent
-            # chain (block argmin -> row load -> neighbour updates -> owner warp's rescan) whose latency, not
-            # bandwidth, sets the pace; the modelled bytes against HBM show how far from a memory bound it runs
+            # the sparse wide descents: per move one bitset row and the moved vertex's neighbours; the SMs holding
+            # a slot issue on ~2/3 of their cycles with half the lanes idle (divergent neighbour loops), so
+            # instruction issue, not bandwidth, sets the pace; the modelled bytes against HBM show how far from a
+            # memory bound it runs
             roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_descent_wide_sparse",
                         "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": descent_ms,
-                        "limiter": "latency of the per-move chain (block argmin, bitset row, neighbour updates, "
-                                   "rescan); the slot's state "
+                        "limiter": "instruction issue under divergence (0.69 issue per active cycle, 16.8 of 32 "
+                                   "lanes; profiles/k_descent_wide2_sparse_n65536.txt); the slot's state "
                                    + ("in shared memory" if " in shared memory," in plan else "in L2"),
                         "ns_per_move_per_slot": descent_ms * 1e6 / max(moves_per_launch / pop, 1.0)}
         else:
@@ -874,6 +875,27 @@ def main():
                            "timing": "its own solver time (PbilsResult.seconds, best of 3 runs; includes its "
                                      "per-call allocation and bitset upload)",
                            "ours_over_reference": value / (cfg["iterations"] / t_ref)}
+        if args.workload in ("wide2", "wide3") and not args.no_cpu_baseline:
+            # the reference's GPU design at W: a short run of both binaries through their one-call entry points
+            # (5 iterations, same seed; both times include the per-call set-up and the 512 MiB bitset upload)
+            short = 5
+            got = reference_gpu_run(dict(cfg, seed=seed, iterations=short, early_stop=short), runs=1)
+            if got is not None:
+                t_ref, f_ref = got
+                p_short = ccb.PbilsParams(k=cfg["k"], population=cfg["population"], tournament=cfg["tournament"],
+                                          perturbation=cfg["perturbation"], gww=cfg["gww"], iterations=short,
+                                          early_stop=short, seed=seed)
+                t0 = time.perf_counter()
+                r_short = ccb.SolveGpu(g_pinned, p_short)
+                t_ours = time.perf_counter() - t0
+                ref_gpu = {"value": short / t_ref, "unit": "iter/s", "objective": f_ref,
+                           "same_objective": f_ref == r_short.objective, "iterations": short,
+                           "ours_same_run": short / t_ours,
+                           "binary": "oracle/_ref/cc_gpu_ref: the reference's cuda/ sources built for sm_100a",
+                           "timing": "reference: its own solver time (PbilsResult.seconds, one run); ours: wall "
+                                     "time of ccb_pbils_solve from the pinned host bitset; both include the "
+                                     "per-call set-up and the bitset upload",
+                           "ours_over_reference": t_ref / t_ours}
         line = {
             "metric": "PBILS iter/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,

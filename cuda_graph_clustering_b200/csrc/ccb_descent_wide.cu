@@ -36,12 +36,12 @@ cudaError_t Wide2Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st
   return cudaErrorInvalidValue;  // a shared-memory state this large does not fit
 }
 
-template <int W, bool kSmem24>
+template <int W, bool kSmem26>
 cudaError_t GoWide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st) {
-  auto kernel = k_descent_wide3_sparse<1024, W, kSmem24>;
+  auto kernel = k_descent_wide3_sparse<1024, W, kSmem26>;
   size_t smem = 0;
-  if (kSmem24) {
-    smem = Wide3Smem24Bytes(a.gr.n);
+  if (kSmem26) {
+    smem = Wide3Smem26Bytes(a.gr.n);
     const cudaError_t e = RaiseDynamicSmem(kernel, smem);
     if (e != cudaSuccess) return e;
   }
@@ -49,14 +49,14 @@ cudaError_t GoWide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t 
   return cudaGetLastError();
 }
 
-template <bool kSmem24>
+template <bool kSmem26>
 cudaError_t Wide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st) {
   const int words = (a.gr.n + 31) / 32;
   const int per_thread = (words + 1023) / 1024;
-  if (per_thread <= 1) return GoWide3Sparse<1, kSmem24>(a, grid, st);
-  if (per_thread <= 2) return GoWide3Sparse<2, kSmem24>(a, grid, st);
-  if (per_thread <= 4) return GoWide3Sparse<4, kSmem24>(a, grid, st);
-  if constexpr (!kSmem24) {
+  if (per_thread <= 1) return GoWide3Sparse<1, kSmem26>(a, grid, st);
+  if (per_thread <= 2) return GoWide3Sparse<2, kSmem26>(a, grid, st);
+  if (per_thread <= 4) return GoWide3Sparse<4, kSmem26>(a, grid, st);
+  if constexpr (!kSmem26) {
     if (per_thread <= 8) return GoWide3Sparse<8, false>(a, grid, st);
     if (per_thread <= 16) return GoWide3Sparse<16, false>(a, grid, st);
     return GoWide3Sparse<32, false>(a, grid, st);
@@ -67,7 +67,7 @@ cudaError_t Wide3Sparse(const DescentArgs<int32_t>& a, int grid, cudaStream_t st
 }  // namespace
 
 size_t Wide2Smem16Bytes(int n) { return ((size_t)n * 2 + 15) / 16 * 16; }
-size_t Wide3Smem24Bytes(int n) { return ((size_t)n * 3 + 15) / 16 * 16 + 16; }
+size_t Wide3Smem26Bytes(int n) { return (size_t)((n + 31) / 32) * 104 + 16; }  // 26 words per row word
 
 cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& a, int grid, bool sparse, bool smem16,
                                     cudaStream_t st) {

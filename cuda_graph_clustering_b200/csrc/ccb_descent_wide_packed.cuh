@@ -504,37 +504,46 @@ __device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, ui
 }
 
 // Where a k = 3 slot keeps its vertex words.  Wide3Global: the 64-bit words (three 20-bit counters + label) in
-// the slot's rows of `next` (global memory, L2).  Wide3Smem24: a 24-bit record per vertex in shared memory (G1 and
-// G2 in 11 bits each, the label in 2; G0 = degree - G1 - G2), exact while every degree is below 2048; the record
-// of vertex u sits at byte 3u, so the 32 vertices of a row word q fill the 24 words [24q, 24q + 24) and every
-// thread writes only words of its own.  Both present the same 64-bit word to the descent.
+// the slot's rows of `next` (global memory, L2).  Wide3Smem26: a 26-bit record per vertex in shared memory, the
+// label a and the two foreign differences d_c = G_c - G_a (lower foreign cluster first) as 12-bit values offset
+// by 2048, exact while every degree is below 2048 (|d| <= degree).  The descent only ever needs these differences,
+// so the record holds no degree and a load touches shared memory only.  The record of vertex u sits at bit 26u:
+// the 32 vertices of a row word q fill exactly the 26 words [26q, 26q + 26), so every thread writes only words
+// of its own.  Both present a 64-bit word of three 20-bit counters + label to the descent; Wide3Smem26's has
+// G_a = 2^19 and G_c = 2^19 + d_c (the same differences; a move's +-1 steps stay inside the fields), and its
+// store takes the differences of whatever word it is given, re-based on that word's label.
 struct Wide3Global {
   unsigned long long* p;
   __device__ __forceinline__ unsigned long long Load(int u) const { return p[u]; }
   __device__ __forceinline__ void Store(int u, unsigned long long w) const { p[u] = w; }
 };
 
-struct Wide3Smem24 {
+struct Wide3Smem26 {
   uint32_t* words;
-  const int32_t* degrees;
+  static constexpr uint32_t kMask = (1u << 26) - 1u;
+  static constexpr unsigned long long kBase = 1ull << 19;
   __device__ __forceinline__ unsigned long long Load(int u) const {
-    const int o = 3 * u;
-    const int wi = o >> 2, sh = (o & 3) * 8;
+    const int o = 26 * u;
+    const int wi = o >> 5, sh = o & 31;
     uint32_t rec = words[wi] >> sh;
-    if (sh >= 16) rec |= words[wi + 1] << (32 - sh);
-    rec &= 0xFFFFFFu;
-    const unsigned long long g1 = rec & 2047u, g2 = (rec >> 11) & 2047u, label = rec >> 22;
-    const unsigned long long g0 = static_cast<unsigned long long>(degrees[u]) - g1 - g2;
-    return g0 | g1 << 20 | g2 << 40 | label << 60;
+    if (sh > 6) rec |= words[wi + 1] << (32 - sh);
+    rec &= kMask;
+    const int a = static_cast<int>(rec >> 24);
+    const int clo = a == 0 ? 1 : 0, chi = a == 2 ? 1 : 2;
+    const unsigned long long glo = kBase + (rec & 4095u) - 2048u, ghi = kBase + ((rec >> 12) & 4095u) - 2048u;
+    return kBase << (20 * a) | glo << (20 * clo) | ghi << (20 * chi) | static_cast<unsigned long long>(a) << 60;
   }
   __device__ __forceinline__ void Store(int u, unsigned long long w) const {
-    const uint32_t rec = static_cast<uint32_t>((w >> 20) & 2047u) | static_cast<uint32_t>((w >> 40) & 2047u) << 11 |
-                         static_cast<uint32_t>(w >> 60) << 22;
-    const int o = 3 * u;
-    const int wi = o >> 2, sh = (o & 3) * 8;
-    words[wi] = (words[wi] & ~(0xFFFFFFu << sh)) | (rec << sh);
-    if (sh >= 16) {
-      const uint32_t hi_mask = 0xFFFFFFu >> (32 - sh);
+    const int a = static_cast<int>(w >> 60);
+    const int ga = Wide3G(w, a);
+    const int clo = a == 0 ? 1 : 0, chi = a == 2 ? 1 : 2;
+    const uint32_t rec = static_cast<uint32_t>(Wide3G(w, clo) - ga + 2048) |
+                         static_cast<uint32_t>(Wide3G(w, chi) - ga + 2048) << 12 | static_cast<uint32_t>(a) << 24;
+    const int o = 26 * u;
+    const int wi = o >> 5, sh = o & 31;
+    words[wi] = (words[wi] & ~(kMask << sh)) | (rec << sh);
+    if (sh > 6) {
+      const uint32_t hi_mask = kMask >> (32 - sh);
       words[wi + 1] = (words[wi + 1] & ~hi_mask) | (rec >> (32 - sh));
     }
   }
@@ -558,11 +567,11 @@ __device__ __forceinline__ void WarpRescanWide3(const State& state, int n, int w
   }
 }
 
-template <int T, int W, bool kSmem24>
+template <int T, int W, bool kSmem26>
 __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a, int slot) {
   using Key = unsigned long long;
   using Word = unsigned long long;
-  using State = typename std::conditional<kSmem24, Wide3Smem24, Wide3Global>::type;
+  using State = typename std::conditional<kSmem26, Wide3Smem26, Wide3Global>::type;
   constexpr int kWarps = T / kWarp;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
@@ -594,8 +603,8 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
   const int w = s_winner;
 
   State state;
-  if constexpr (kSmem24) {
-    state = State{reinterpret_cast<uint32_t*>(smem), a.gr.degrees};
+  if constexpr (kSmem26) {
+    state = State{reinterpret_cast<uint32_t*>(smem)};
   } else {
     state = State{reinterpret_cast<Word*>(a.next.g + static_cast<size_t>(slot) * a.k * ld)};
   }
@@ -603,8 +612,8 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
   {
     const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
     const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
-    if constexpr (kSmem24) {
-      // a thread writes the vertices of its own row words only (the 24-bit records of a word's 32 vertices share
+    if constexpr (kSmem26) {
+      // a thread writes the vertices of its own row words only (the 26-bit records of a word's 32 vertices share
       // memory words with nothing else): the vertices of word q = word0 + 32 i are written by this thread
 #pragma unroll 1
       for (int i = 0; i < W; ++i) {
@@ -769,9 +778,9 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
   }
 }
 
-template <int T, int W, bool kSmem24>
+template <int T, int W, bool kSmem26>
 __global__ void __launch_bounds__(T, 1) k_descent_wide3_sparse(DescentArgs<int32_t> a) {
-  DescentWide3Sparse<T, W, kSmem24>(a, blockIdx.x);
+  DescentWide3Sparse<T, W, kSmem26>(a, blockIdx.x);
 }
 
 }  // namespace ccb

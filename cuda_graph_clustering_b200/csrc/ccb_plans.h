@@ -46,11 +46,11 @@ cudaError_t LaunchDescentIncrementalWide(const DescentArgs<int32_t>& args, int g
 // With `sparse`: the degree-proportional forms (per-thread best vertex of each cluster, k = 2, or of each
 // (cluster, target) class, k = 3).
 // With `smem16` the sparse forms keep the slot's words in shared memory: k = 2 as int16 (Wide2Smem16Bytes(n)
-// bytes, every degree below 16384), k = 3 as 24-bit records (Wide3Smem24Bytes(n) bytes, every degree below 2048).
+// bytes, every degree below 16384), k = 3 as 26-bit records (Wide3Smem26Bytes(n) bytes, every degree below 2048).
 cudaError_t LaunchDescentWidePacked(const DescentArgs<int32_t>& args, int grid, bool sparse, bool smem16,
                                     cudaStream_t stream);
 size_t Wide2Smem16Bytes(int n);
-size_t Wide3Smem24Bytes(int n);
+size_t Wide3Smem26Bytes(int n);
 cudaError_t LaunchDescentSmallK(const SmallKPlan& plan, const DescentArgs<int16_t>& args, int grid,
                                 cudaStream_t stream, bool configure);
 

@@ -167,7 +167,7 @@ struct Plan {
   bool incremental = false; // the incremental 9 <= k <= 64 descent
   bool packed_wide = false;  // the packed wide descent (k = 2, 3)
   bool sparse = false;       // k = 2 packed wide: the degree-proportional form (sparse graphs)
-  bool smem16 = false;       // sparse k = 2 / 3: the slot's words in shared memory (int16 / 24-bit records)
+  bool smem16 = false;       // sparse k = 2 / 3: the slot's words in shared memory (int16 / 26-bit records)
   SmallKPlan sk;
 };
 
@@ -367,7 +367,7 @@ const char* KernelName(const Plan& p) {
   if (p.packed_wide) {
     if (p.sk.k == 3) {
       if (p.smem16) return "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), "
-                           "24-bit records in shared memory";
+                           "26-bit records in shared memory";
       return p.sparse ? "packed wide k = 3, degree-proportional (per-thread best of each (cluster, target) class), L2"
                       : "packed wide k = 3 (three 20-bit counters and the label, 8 bytes per vertex), L2";
     }
@@ -528,12 +528,12 @@ int MaxDegree(const ccb_graph& g) {
 }
 
 // The sparse wide descents keep the slot's words in shared memory when they fit: k = 2 as int16 (2e + label) when
-// every degree is below 16384 (|2e + 1| < 2^15), k = 3 as 24-bit records (two 11-bit counters and the label) when
-// every degree is below 2048; else in global memory (int32 / 64-bit words).
+// every degree is below 16384 (|2e + 1| < 2^15), k = 3 as 26-bit records (the label and two 12-bit counter
+// differences) when every degree is below 2048; else in global memory (int32 / 64-bit words).
 void PlanSmem16(ccb_solver& s) {
   s.plan.smem16 = false;
   if (!(s.plan.packed_wide && s.plan.sparse && (s.k == 2 || s.k == 3))) return;
-  const size_t bytes = s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem24Bytes(s.n);
+  const size_t bytes = s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem26Bytes(s.n);
   if (bytes + 4096 > (size_t)s.device.smem_optin) return;
   s.plan.smem16 = MaxDegree(*s.graph) < (s.k == 2 ? 16384 : 2048);
 }
@@ -542,7 +542,7 @@ void PlanSmem16(ccb_solver& s) {
 void Describe(ccb_solver& s) {
   char text[320];
   // the sparse wide descents size their own shared state at launch (the slot's words when they fit)
-  const size_t smem = s.plan.smem16 ? (s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem24Bytes(s.n)) : s.plan.smem_bytes;
+  const size_t smem = s.plan.smem16 ? (s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem26Bytes(s.n)) : s.plan.smem_bytes;
   std::snprintf(text, sizeof(text), "%s, %d threads per block, %d blocks, %zu bytes of shared memory%s",
                 KernelName(s.plan), s.plan.threads, s.pop * std::max(1, s.plan.sk.cluster), smem,
                 s.tensor ? "; G rebuilt on the tensor cores (int8 tcgen05, TMA)" : "");
