@@ -219,31 +219,25 @@ __global__ void __launch_bounds__(T, 1) k_descent_wide_packed(DescentArgs<int32_
 // thread's best), in the other they get worse (the thread rescans its vertices only if its best was among
 // them), and v changes cluster.  A thread owns the row words {32 W j + 32 i + lane : i < W} of its warp's
 // stretch (W words per thread), so the row of v is read coalesced and a rescan reads 128-byte runs.
-struct WideBest2 {
-  int e0, u0;  // cluster 0: largest e, lowest vertex (u0 < 0: none)
-  int e1, u1;  // cluster 1: smallest e, lowest vertex
-  __device__ void Clear() {
-    e0 = e1 = 0;
-    u0 = u1 = -1;
-  }
-  __device__ void Offer(int w, int u) {
-    const int e = w >> 1;
-    if (w & 1) {
-      if (u1 < 0 || e < e1 || (e == e1 && u < u1)) e1 = e, u1 = u;
-    } else {
-      if (u0 < 0 || e > e0 || (e == e0 && u < u0)) e0 = e, u0 = u;
-    }
-  }
-};
+// Best moves of the sparse k = 2 descent, one pair per thread (the owner of whole row words), kept in shared
+// memory so that any lane of the owner's warp can improve them: cluster 0's best is the largest
+// (e + 2^20) << 11 | (2047 - j) over the owner's cluster-0 vertices (largest e, then lowest vertex), cluster 1's the
+// smallest (e + 2^20) << 11 | j over its cluster-1 vertices (smallest e, then lowest vertex), with j = 32 i + bit the
+// vertex's place among the owner's (word i of the owner, lower j = lower vertex); 0 and ~0 mean none (e > -2^20
+// keeps both out of reach).
+__device__ __forceinline__ uint32_t Wide2Key0(int wd, uint32_t j) {
+  return static_cast<uint32_t>((wd >> 1) + (1 << 20)) << 11 | (2047u - j);
+}
+__device__ __forceinline__ uint32_t Wide2Key1(int wd, uint32_t j) {
+  return static_cast<uint32_t>((wd >> 1) + (1 << 20)) << 11 | j;
+}
 
-// Recomputes lane `owner`'s two bests with the whole warp: the owner's vertices are the 32 of each of its row
-// words, lane l reads vertex l of every word (128-byte runs), and two warp reductions pick the best of each
-// cluster.  Keys: cluster 0 max of (e + 2^20) << 11 | (2047 - j), cluster 1 min of (e + 2^20) << 11 | j, with
-// j = 32 i + lane the vertex's place among the owner's (lower j = lower vertex); e > -2^20 keeps both
-// sentinels (0 and ~0) out of reach.
+// Recomputes lane `owner`'s two best keys with the whole warp: the owner's vertices are the 32 of each of its row
+// words, lane l reads vertex l of every word (128-byte runs), two warp reductions pick the best of each cluster,
+// and the owner stores them.
 template <int W, typename StateT>
 __device__ __forceinline__ void WarpRescanWide2(const StateT* state, int n, int words, int owner_word0, int owner,
-                                                WideBest2& b) {
+                                                uint32_t* k0_out, uint32_t* k1_out) {
   const int lane = threadIdx.x % kWarp;
   uint32_t k0 = 0u, k1 = ~0u;
 #pragma unroll(W < 8 ? W : 8)
@@ -253,43 +247,48 @@ __device__ __forceinline__ void WarpRescanWide2(const StateT* state, int n, int 
     if (q < words && u < n) {
       const int wd = state[u];
       const uint32_t j = static_cast<uint32_t>(i * kWarp + lane);
-      const uint32_t e = static_cast<uint32_t>((wd >> 1) + (1 << 20));
       if (wd & 1) {
-        k1 = min(k1, e << 11 | j);
+        k1 = min(k1, Wide2Key1(wd, j));
       } else {
-        k0 = max(k0, e << 11 | (2047u - j));
+        k0 = max(k0, Wide2Key0(wd, j));
       }
     }
   }
   k0 = __reduce_max_sync(kAllLanes, k0);
   k1 = __reduce_min_sync(kAllLanes, k1);
   if (lane == owner) {
-    b.Clear();
-    if (k0 != 0u) {
-      const int j = 2047 - static_cast<int>(k0 & 2047u);
-      b.e0 = static_cast<int>(k0 >> 11) - (1 << 20);
-      b.u0 = 32 * (owner_word0 + (j / kWarp) * kWarp) + j % kWarp;
-    }
-    if (k1 != ~0u) {
-      const int j = static_cast<int>(k1 & 2047u);
-      b.e1 = static_cast<int>(k1 >> 11) - (1 << 20);
-      b.u1 = 32 * (owner_word0 + (j / kWarp) * kWarp) + j % kWarp;
-    }
+    *k0_out = k0;
+    *k1_out = k1;
   }
 }
 
 // kSmem16: the slot's words 2e + label as int16 in shared memory (n * 2 bytes), exact while every degree is below
 // 16384 (|2e + label| <= 2 deg + 1 < 2^15); else int32 in the slot's rows of `next` (global memory, L2).  Every
-// thread reads and writes only its own vertices' words, so the two placements run the same code.
+// vertex belongs to the thread that owns its row word; the two placements run the same code.
+//
+// Per move the neighbours of the moved vertex v are processed by the whole warp rather than each owner alone (a
+// thread holds about one neighbour per move at p = 0.02, so per-thread loops left most lanes idle): the warp
+// writes the set bits of its row words into a short list (owner, word, bit) in shared memory, in rounds of
+// kWide2List entries, and its lanes take the entries in turn.  A neighbour's word changes by +-4 (e +- 2); if that
+// makes it better, its owner's key is improved with a shared-memory atomic max / min; if worse and it was the
+// owner's best, the owner is flagged and the warp rescans the owner's vertices after the round.  Keys, ties and
+// the order of moves are those of the per-thread form (largest / smallest e, then the lowest vertex).
+constexpr int kWide2List = 128;  // list entries per warp and round
+
 template <int T, int W, bool kSmem16>
 __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a, int slot) {
   using Key = unsigned long long;
   using StateT = typename std::conditional<kSmem16, int16_t, int32_t>::type;
   constexpr int kWarps = T / kWarp;
+  static_assert(W <= 32, "list entries hold the word index in 5 bits");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_winner;
   __shared__ int s_stop;
   __shared__ MoveRecord<Key> s_records[2 * kWarps];
+  __shared__ uint32_t s_k0[T];       // each thread's best key of cluster 0 (largest)
+  __shared__ uint32_t s_k1[T];       // and of cluster 1 (smallest)
+  __shared__ uint8_t s_rescan[T];    // the thread's best of the worsened cluster was a neighbour of the move
+  __shared__ uint16_t s_list[kWarps][kWide2List];
 
   const int tid = threadIdx.x;
   const int lane = tid % kWarp;
@@ -299,7 +298,8 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
   const int bits = a.key_bits;
   const int pitch = a.gr.pitch;
   const int words = (n + 31) / 32;
-  const int word0 = warp * kWarp * W + lane;  // this thread's row words: word0 + 32 i, i < W
+  const int warp_word0 = warp * kWarp * W;  // the warp's row words: warp_word0 + lane + 32 i, i < W
+  const int word0 = warp_word0 + lane;      // this thread's row words: word0 + 32 i, i < W
 
   if (tid == 0) {
     s_stop = a.ctl->stop;
@@ -310,19 +310,17 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
                                   : slot;
     }
   }
+  s_rescan[tid] = 0;
   __syncthreads();
   if (s_stop) return;
   const int w = s_winner;
 
   StateT* state = kSmem16 ? reinterpret_cast<StateT*>(smem)
                           : reinterpret_cast<StateT*>(a.next.g + static_cast<size_t>(slot) * a.k * ld);
-  WideBest2 b;
-  b.Clear();
   {
     const int32_t* g = a.cur.g + static_cast<size_t>(w) * a.k * ld;
     const uint8_t* lab = a.cur.labels + static_cast<size_t>(w) * ld;
     // the warp builds its owners' words 32 at a time (vertex 32 q + lane of each of its words q)
-    const int warp_word0 = warp * kWarp * W;
 #pragma unroll 1
     for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
       const int u = 32 * q + lane;
@@ -330,7 +328,11 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
     }
     __syncwarp();
 #pragma unroll 1
-    for (int owner = 0; owner < kWarp; ++owner) WarpRescanWide2<W>(state, n, words, warp_word0 + owner, owner, b);
+    for (int owner = 0; owner < kWarp; ++owner) {
+      WarpRescanWide2<W>(state, n, words, warp_word0 + owner, owner, &s_k0[warp * kWarp + owner],
+                         &s_k1[warp * kWarp + owner]);
+    }
+    __syncwarp();
   }
   const int32_t* sizes = a.cur.sizes + static_cast<size_t>(w) * a.kpad;
   int s = sizes[1] - sizes[0];
@@ -343,17 +345,24 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
   while (true) {
     Key best = KeyTraits<Key>::kNone;
     uint32_t payload = 0;
-    if (b.u0 >= 0) {
-      const int gain = s + 1 - 2 * b.e0;
+    const uint32_t k0 = s_k0[tid], k1 = s_k1[tid];
+    if (k0 != 0u) {  // this thread's best move out of cluster 0
+      const int e0 = static_cast<int>(k0 >> 11) - (1 << 20);
+      const int j = 2047 - static_cast<int>(k0 & 2047u);
+      const int u0 = 32 * (word0 + (j / kWarp) * kWarp) + j % kWarp;
+      const int gain = s + 1 - 2 * e0;
       if (gain < 0) {
-        best = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(b.u0);
+        best = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(u0);
         payload = 0u | 1u << 8;
       }
     }
-    if (b.u1 >= 0) {
-      const int gain = 1 - s + 2 * b.e1;
+    if (k1 != ~0u) {  // and out of cluster 1
+      const int e1 = static_cast<int>(k1 >> 11) - (1 << 20);
+      const int j = static_cast<int>(k1 & 2047u);
+      const int u1 = 32 * (word0 + (j / kWarp) * kWarp) + j % kWarp;
+      const int gain = 1 - s + 2 * e1;
       if (gain < 0) {
-        const Key mk = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(b.u1);
+        const Key mk = (static_cast<Key>(gain + (1 << bits)) << bits) + static_cast<Key>(u1);
         if (mk < best) {
           best = mk;
           payload = 1u;
@@ -376,79 +385,100 @@ __device__ __forceinline__ void DescentWide2Sparse(const DescentArgs<int32_t>& a
     const int step = to == 1 ? 4 : -4;
     const int worse = to;  // e up hurts cluster 1 (smallest e wanted), e down hurts cluster 0
     const uint32_t* row = a.gr.bits + static_cast<size_t>(v) * pitch;
-    bool rescan = false;
+    uint16_t* list = s_list[warp];
     constexpr int kChunk = W < 4 ? W : 4;  // row words in flight together (one memory latency per chunk)
 #pragma unroll 1
     for (int i0 = 0; i0 < W; i0 += kChunk) {
-      uint32_t rwords[kChunk];
+      uint32_t rw[kChunk];
 #pragma unroll
       for (int t = 0; t < kChunk; ++t) {
         const int q = word0 + (i0 + t) * kWarp;
-        rwords[t] = q < words ? row[q] : 0u;
+        rw[t] = q < words ? row[q] : 0u;
       }
-      // two row words at a time as one 64-bit mask (word i in the low half, word i + 1 in the high half): a
-      // thread holds about one neighbour per pair at p = 0.02, so one batch of four usually covers both words
+      int cnt = 0;
 #pragma unroll
-      for (int t = 0; t < kChunk; t += 2) {
-        const int i = i0 + t;
-        unsigned long long mbits = rwords[t];
-        if (t + 1 < kChunk) mbits |= static_cast<unsigned long long>(rwords[t + 1]) << 32;
-        const int base = 32 * (word0 + i * kWarp);
-        while (mbits) {
-          // up to four neighbours with their loads in flight together
-          int us[4];
-          int ws[4];
+      for (int t = 0; t < kChunk; ++t) cnt += __popc(rw[t]);
+      int incl = cnt;  // inclusive prefix of the lanes' neighbour counts
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            us[c] = -1;
-            if (mbits) {
-              const int bit = __ffsll(mbits) - 1;
-              us[c] = base + (bit >> 5) * (32 * kWarp) + (bit & 31);
-              mbits &= mbits - 1;
-            }
-          }
+      for (int o = 1; o < kWarp; o <<= 1) {
+        const int y = __shfl_up_sync(kAllLanes, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int total = __shfl_sync(kAllLanes, incl, kWarp - 1);
+      int pos = incl - cnt;  // this lane's next list position (its entries are [incl - cnt, incl))
+#pragma unroll 1
+      for (int r0 = 0; r0 < total; r0 += kWide2List) {
+        const int r1 = r0 + kWide2List;
 #pragma unroll
-          for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state[us[c]] : 0;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            if (us[c] < 0) continue;
-            const int wd = ws[c] + step;
-            state[us[c]] = static_cast<StateT>(wd);
-            if ((wd & 1) == worse) {
-              rescan |= us[c] == ((wd & 1) ? b.u1 : b.u0);
-            } else {
-              b.Offer(wd, us[c]);
-            }
+        for (int t = 0; t < kChunk; ++t) {
+          while (rw[t] != 0u && pos < r1) {
+            const int bit = __ffs(rw[t]) - 1;
+            rw[t] &= rw[t] - 1;
+            list[pos - r0] = static_cast<uint16_t>(lane << 10 | (i0 + t) << 5 | bit);
+            ++pos;
           }
         }
+        __syncwarp();
+        const int here = min(kWide2List, total - r0);
+        for (int p = lane; p < here; p += kWarp) {
+          const int entry = list[p];
+          const int owner = entry >> 10, i = (entry >> 5) & 31, bit = entry & 31;
+          const int u = 32 * (warp_word0 + owner + i * kWarp) + bit;
+          const uint32_t j = static_cast<uint32_t>(i * kWarp + bit);
+          const int otid = warp * kWarp + owner;
+          const int wd = state[u] + step;
+          state[u] = static_cast<StateT>(wd);
+          if ((wd & 1) == worse) {  // u got worse: a rescan of its owner if u was the owner's best
+            if (wd & 1) {
+              const uint32_t kb = s_k1[otid];
+              if (kb != ~0u && (kb & 2047u) == j) s_rescan[otid] = 1;
+            } else {
+              const uint32_t kb = s_k0[otid];
+              if (kb != 0u && (kb & 2047u) == 2047u - j) s_rescan[otid] = 1;
+            }
+          } else if (wd & 1) {  // u got better: it may become its owner's best
+            atomicMin(&s_k1[otid], Wide2Key1(wd, j));
+          } else {
+            atomicMax(&s_k0[otid], Wide2Key0(wd, j));
+          }
+        }
+        __syncwarp();
       }
     }
     // v itself changes cluster (its e is unchanged: no self-loops)
     const int qv = v >> 5;
-    if (qv >= warp * kWarp * W && qv < (warp + 1) * kWarp * W && (qv - warp * kWarp * W) % kWarp == lane) {
+    bool rescan = false;
+    if (qv >= warp_word0 && qv < warp_word0 + kWarp * W && (qv - warp_word0) % kWarp == lane) {
       const int wd = state[v] ^ 1;
       state[v] = static_cast<StateT>(wd);
-      rescan |= v == (to == 1 ? b.u0 : b.u1);
-      b.Offer(wd, v);
+      const uint32_t jv = static_cast<uint32_t>(((qv - warp_word0) / kWarp) * kWarp + (v & 31));
+      if (to == 1) {  // v left cluster 0 and joins cluster 1
+        rescan = s_k0[tid] != 0u && (s_k0[tid] & 2047u) == 2047u - jv;
+        s_k1[tid] = min(s_k1[tid], Wide2Key1(wd, jv));
+      } else {
+        rescan = s_k1[tid] != ~0u && (s_k1[tid] & 2047u) == jv;
+        s_k0[tid] = max(s_k0[tid], Wide2Key0(wd, jv));
+      }
     }
-    __syncwarp();  // every lane's stores are visible to the warp's rescans
+    __syncwarp();  // every lane's stores and flags are visible to the warp's rescans
+    rescan |= s_rescan[tid] != 0;
+    s_rescan[tid] = 0;
     unsigned pending = __ballot_sync(kAllLanes, rescan);
     while (pending) {
       const int owner = __ffs(pending) - 1;
       pending &= pending - 1;
-      WarpRescanWide2<W>(state, n, words, warp * kWarp * W + owner, owner, b);
+      WarpRescanWide2<W>(state, n, words, warp_word0 + owner, owner, &s_k0[warp * kWarp + owner],
+                         &s_k1[warp * kWarp + owner]);
     }
+    __syncwarp();
   }
 
   __syncwarp();
   uint8_t* dst = a.next.labels + static_cast<size_t>(slot) * ld;
-  {
-    const int warp_word0 = warp * kWarp * W;
 #pragma unroll 1
-    for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
-      const int u = 32 * q + lane;
-      if (u < n) dst[u] = static_cast<uint8_t>(state[u] & 1);
-    }
+  for (int q = warp_word0; q < min(words, warp_word0 + kWarp * W); ++q) {
+    const int u = 32 * q + lane;
+    if (u < n) dst[u] = static_cast<uint8_t>(state[u] & 1);
   }
   if (tid == 0) {
     a.next.f[slot] = objective;

@@ -534,7 +534,8 @@ void PlanSmem16(ccb_solver& s) {
   s.plan.smem16 = false;
   if (!(s.plan.packed_wide && s.plan.sparse && (s.k == 2 || s.k == 3))) return;
   const size_t bytes = s.k == 2 ? Wide2Smem16Bytes(s.n) : Wide3Smem26Bytes(s.n);
-  if (bytes + 4096 > (size_t)s.device.smem_optin) return;
+  // room beside the state for the kernel's static shared memory (k = 2: per-thread keys and neighbour lists, ~18 KB)
+  if (bytes + (s.k == 2 ? 24 * 1024 : 4096) > (size_t)s.device.smem_optin) return;
   s.plan.smem16 = MaxDegree(*s.graph) < (s.k == 2 ? 16384 : 2048);
 }
 
