@@ -524,12 +524,34 @@ __device__ __forceinline__ Wide3Keys Wide3KeysOf(unsigned long long wd, uint32_t
 }
 
 // Folds vertex word wd (place j) into the keys of its two classes.  The six keys are indexed by compile-time
-// class only (a predicate per class) so that they stay in registers.
+// class only (one branch per cluster) so that they stay in registers.
 __device__ __forceinline__ void Wide3Offer(unsigned long long wd, uint32_t j, uint32_t (&key)[6]) {
   const Wide3Keys kk = Wide3KeysOf(wd, j);
-#pragma unroll
-  for (int cls = 0; cls < 6; ++cls) {
-    if ((cls >> 1) == kk.a) key[cls] = max(key[cls], (cls & 1) ? kk.hi : kk.lo);
+  if (kk.a == 0) {
+    key[0] = max(key[0], kk.lo);
+    key[1] = max(key[1], kk.hi);
+  } else if (kk.a == 1) {
+    key[2] = max(key[2], kk.lo);
+    key[3] = max(key[3], kk.hi);
+  } else {
+    key[4] = max(key[4], kk.lo);
+    key[5] = max(key[5], kk.hi);
+  }
+}
+
+// A neighbour's change to its two class keys (lower and higher foreign target): better (dl / dh > 0) raises the
+// key, worse (< 0) asks for a rescan when the class's best is this vertex (tail = 2047 - its place).
+__device__ __forceinline__ void Wide3Fold(uint32_t& klo, uint32_t& khi, const Wide3Keys& kk, int dl, int dh,
+                                          uint32_t tail, bool& rescan) {
+  if (dl > 0) {
+    klo = max(klo, kk.lo);
+  } else if (dl < 0) {
+    rescan |= (klo & 2047u) == tail;
+  }
+  if (dh > 0) {
+    khi = max(khi, kk.hi);
+  } else if (dh < 0) {
+    rescan |= (khi & 2047u) == tail;
   }
 }
 
@@ -758,16 +780,16 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
             const Wide3Keys kk = Wide3KeysOf(wd, j);
             const int au = kk.a;
             const int own = (au == from) - (au == to);
-#pragma unroll
-            for (int cls = 0; cls < 6; ++cls) {
-              if ((cls >> 1) != au) continue;
-              const int cc = (cls & 1) ? (au == 2 ? 1 : 2) : (au == 0 ? 1 : 0);
-              const int delta = (cc == to) - (cc == from) + own;
-              if (delta > 0) {
-                key[cls] = max(key[cls], (cls & 1) ? kk.hi : kk.lo);
-              } else if (delta < 0) {
-                rescan |= (key[cls] & 2047u) == (2047u - j);  // the class's best got worse
-              }
+            const int clo = au == 0 ? 1 : 0, chi = au == 2 ? 1 : 2;
+            const int dl = (clo == to) - (clo == from) + own;  // change of d for the class (au, clo)
+            const int dh = (chi == to) - (chi == from) + own;  // and (au, chi)
+            const uint32_t tail = 2047u - j;
+            if (au == 0) {  // classes 2 au and 2 au + 1
+              Wide3Fold(key[0], key[1], kk, dl, dh, tail, rescan);
+            } else if (au == 1) {
+              Wide3Fold(key[2], key[3], kk, dl, dh, tail, rescan);
+            } else {
+              Wide3Fold(key[4], key[5], kk, dl, dh, tail, rescan);
             }
           }
         }
