@@ -574,12 +574,25 @@ struct Wide3Smem26 {
   uint32_t* words;
   static constexpr uint32_t kMask = (1u << 26) - 1u;
   static constexpr unsigned long long kBase = 1ull << 19;
-  __device__ __forceinline__ unsigned long long Load(int u) const {
+  // The raw record: d_lo + 2048 | (d_hi + 2048) << 12 | a << 24.
+  __device__ __forceinline__ uint32_t LoadRec(int u) const {
     const int o = 26 * u;
     const int wi = o >> 5, sh = o & 31;
     uint32_t rec = words[wi] >> sh;
     if (sh > 6) rec |= words[wi + 1] << (32 - sh);
-    rec &= kMask;
+    return rec & kMask;
+  }
+  __device__ __forceinline__ void StoreRec(int u, uint32_t rec) const {
+    const int o = 26 * u;
+    const int wi = o >> 5, sh = o & 31;
+    words[wi] = (words[wi] & ~(kMask << sh)) | (rec << sh);
+    if (sh > 6) {
+      const uint32_t hi_mask = kMask >> (32 - sh);
+      words[wi + 1] = (words[wi + 1] & ~hi_mask) | (rec >> (32 - sh));
+    }
+  }
+  __device__ __forceinline__ unsigned long long Load(int u) const {
+    const uint32_t rec = LoadRec(u);
     const int a = static_cast<int>(rec >> 24);
     const int clo = a == 0 ? 1 : 0, chi = a == 2 ? 1 : 2;
     const unsigned long long glo = kBase + (rec & 4095u) - 2048u, ghi = kBase + ((rec >> 12) & 4095u) - 2048u;
@@ -589,15 +602,8 @@ struct Wide3Smem26 {
     const int a = static_cast<int>(w >> 60);
     const int ga = Wide3G(w, a);
     const int clo = a == 0 ? 1 : 0, chi = a == 2 ? 1 : 2;
-    const uint32_t rec = static_cast<uint32_t>(Wide3G(w, clo) - ga + 2048) |
-                         static_cast<uint32_t>(Wide3G(w, chi) - ga + 2048) << 12 | static_cast<uint32_t>(a) << 24;
-    const int o = 26 * u;
-    const int wi = o >> 5, sh = o & 31;
-    words[wi] = (words[wi] & ~(kMask << sh)) | (rec << sh);
-    if (sh > 6) {
-      const uint32_t hi_mask = kMask >> (32 - sh);
-      words[wi + 1] = (words[wi + 1] & ~hi_mask) | (rec >> (32 - sh));
-    }
+    StoreRec(u, static_cast<uint32_t>(Wide3G(w, clo) - ga + 2048) |
+                    static_cast<uint32_t>(Wide3G(w, chi) - ga + 2048) << 12 | static_cast<uint32_t>(a) << 24);
   }
 };
 
@@ -757,7 +763,8 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
         while (mbits) {
           int us[4];
           uint32_t js[4];  // the vertex's place among the thread's: (word index) * 32 + bit
-          Word ws[4];
+          Word ws[4];      // 64-bit counter words (state in global memory)
+          uint32_t rs[4];  // or the raw 26-bit records (shared memory)
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             us[c] = -1;
@@ -770,20 +777,39 @@ __device__ __forceinline__ void DescentWide3Sparse(const DescentArgs<int32_t>& a
             }
           }
 #pragma unroll
-          for (int c = 0; c < 4; ++c) ws[c] = us[c] >= 0 ? state.Load(us[c]) : Word{};
+          for (int c = 0; c < 4; ++c) {
+            if constexpr (kSmem26) {
+              rs[c] = us[c] >= 0 ? state.LoadRec(us[c]) : 0u;
+            } else {
+              ws[c] = us[c] >= 0 ? state.Load(us[c]) : Word{};
+            }
+          }
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             if (us[c] < 0) continue;
-            const Word wd = ws[c] + step;
-            state.Store(us[c], wd);
             const uint32_t j = js[c];
-            const Wide3Keys kk = Wide3KeysOf(wd, j);
+            const uint32_t tail = 2047u - j;
+            Wide3Keys kk;
+            if constexpr (kSmem26) {
+              kk.a = static_cast<int>(rs[c] >> 24);
+            } else {
+              const Word wd = ws[c] + step;
+              state.Store(us[c], wd);
+              kk = Wide3KeysOf(wd, j);
+            }
             const int au = kk.a;
             const int own = (au == from) - (au == to);
             const int clo = au == 0 ? 1 : 0, chi = au == 2 ? 1 : 2;
             const int dl = (clo == to) - (clo == from) + own;  // change of d for the class (au, clo)
             const int dh = (chi == to) - (chi == from) + own;  // and (au, chi)
-            const uint32_t tail = 2047u - j;
+            if constexpr (kSmem26) {
+              // the record holds the two differences themselves: add the changes in place (|d| <= degree < 2048
+              // keeps both fields inside [1, 4095], so no borrow or carry crosses a field)
+              const uint32_t rec = rs[c] + static_cast<uint32_t>(dl) + (static_cast<uint32_t>(dh) << 12);
+              state.StoreRec(us[c], rec);
+              kk.lo = static_cast<uint32_t>(static_cast<int>(rec & 4095u) - 2048 + (1 << 20)) << 11 | tail;
+              kk.hi = static_cast<uint32_t>(static_cast<int>((rec >> 12) & 4095u) - 2048 + (1 << 20)) << 11 | tail;
+            }
             if (au == 0) {  // classes 2 au and 2 au + 1
               Wide3Fold(key[0], key[1], kk, dl, dh, tail, rescan);
             } else if (au == 1) {
