@@ -828,6 +828,23 @@ def main():
                         "frac": achieved / l2_peak, "traffic": traffic, "kernel": "k_descent",
                         "avg_launch_ms": descent_ms, "peak_kind": "measured L2 copy (profiles/peaks_l2_hbm_int8.txt)",
                         "basis": modelled["basis"], "modelled_bytes": modelled}
+        elif "degree-proportional" in plan and args.workload == "wide2" and \
+                profiled_value("k_descent_wide2_sparse_n65536", "warp_inst_per_move_per_block"):
+            # the W k = 2 descent (int16 state in shared memory): issue roofline with the instructions per move of
+            # its own ncu summary, the modelled bytes beside
+            inst_per_move = profiled_value("k_descent_wide2_sparse_n65536", "warp_inst_per_move_per_block")
+            sm_hz = (clock_info.get("sm_mhz") or 1965.0) * 1e6
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            issue_peak = sms * 4 * sm_hz / 1e9
+            ach = inst_per_move * moves_per_launch / (descent_ms * 1e-3) / 1e9
+            roofline = {"bound": "issue", "achieved": ach, "peak": issue_peak, "unit": "G warp-inst/s",
+                        "frac": ach / issue_peak, "traffic": traffic, "kernel": "k_descent_wide2_sparse",
+                        "avg_launch_ms": descent_ms,
+                        "limiter": "instruction issue under divergence; instructions per move from "
+                                   "profiles/k_descent_wide2_sparse_n65536.txt",
+                        "peak_kind": "issue slots of all SMs (4 per SM per cycle) at the sampled SM clock",
+                        "ns_per_move_per_slot": descent_ms * 1e6 / max(moves_per_launch / pop, 1.0),
+                        "modelled_bytes": modelled}
         elif "degree-proportional" in plan:
             # the sparse wide descents: per move one bitset row and the moved vertex's neighbours; the SMs holding
             # a slot issue on ~2/3 of their cycles with half the lanes idle (divergent neighbour loops), so
