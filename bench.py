@@ -604,7 +604,8 @@ def run_neighborhood(args, rank, world, local):
                        "unit": "G warp-inst/s", "frac": ach / issue_peak if inst_per_move else None,
                        "traffic": profiled_traffic("k_descent_neighborhood"), "kernel": "k_descent_registers",
                        "avg_launch_ms": descent_ms,
-                       "limiter": "latency of the per-move chain; instructions per move from "
+                       "limiter": "instruction issue (72 % of active cycles, ALU pipe 82 % on the SMs in use); "
+                                  "instructions per move from "
                                   "profiles/k_descent_neighborhood.txt",
                        "modelled_bytes": {"achieved_gbs": modelled, "hbm_peak_gbs": peak, "hbm_peak_kind": peak_kind,
                                           "frac_of_hbm": modelled / peak,
